@@ -1,0 +1,354 @@
+"""Benchmark of the B200 PDLP engine on the single large LP of the benchmark
+family: equality-form random LP, m = 500,000 rows, n = 1,000,000 columns,
+8 nonzeros per column (8M nnz), values stored in FP32, solved to 1e-6 relative
+KKT (every answer checked by the engine's device-side restatement of the
+reference verifier). One step = one full solve from a cold start.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Prints ONE JSON line (rank 0). Under torchrun with N > 1 every rank solves its
+own replica of the LP (a single LP does not shard) and `value`
+is the total solves/s of the job, timed as the max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "team-suprema_b200"))
+
+METRIC = "LP solves/s & p50/p99 latency at 1e-6 rel KKT vs plain PDLP; SpMV HBM GB/s"
+UNIT = "solves/s"
+
+WORKLOADS = {
+    # name: (kind, params)
+    "large": ("random", dict(m=500_000, n=1_000_000, k=8, seed=1, fp32=True)),
+    "transport": ("transport", dict(S=2000, D=500, seed=1)),
+    "small": ("random", dict(m=600, n=1800, k=6, seed=0, fp32=False)),
+    "medium": ("random", dict(m=50_000, n=150_000, k=6, seed=3, fp32=True)),
+}
+
+
+def describe(name):
+    kind, p = WORKLOADS[name]
+    if kind == "random":
+        return (f"random equality LP m={p['m']} n={p['n']} {p['k']} nnz/col values "
+                f"{'FP32' if p['fp32'] else 'FP64'} U[-1,1], 0<=x<=10, seed {p['seed']}")
+    return f"transportation LP {p['S']}x{p['D']} (n={p['S'] * p['D']}, m={p['S'] + p['D']}), seed {p['seed']}"
+
+
+def make_lp(B, name):
+    kind, p = WORKLOADS[name]
+    if kind == "random":
+        return B.gen_random_lp(p["m"], p["n"], p["k"], p["seed"], p["fp32"])
+    return B.gen_transport(p["S"], p["D"], p["seed"])
+
+
+def algorithmic_bytes(m, n, z, p):
+    """Per accepted PDHG iteration with p-byte iterates: B_spmv(A) + B_spmv(A^T)
+    + primal pass (read x, A^T y, c, l, u, xsum; write x', xsum) + dual pass
+    (read y, Ax', Ax, b, ysum; write y', ysum); B_spmv = 8Z + 4(R+1) + p C + p R."""
+    spmv_a = 8 * z + 4 * (m + 1) + p * n + p * m
+    spmv_at = 8 * z + 4 * (n + 1) + p * m + p * n
+    return spmv_a + spmv_at + 8 * p * n + 7 * p * m
+
+
+def spmv_bytes(rows, cols, z, p=4):
+    return 8 * z + 4 * (rows + 1) + p * cols + p * rows
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def dist_setup(n_gpus):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import torch
+        import torch.distributed as dist
+        from datetime import timedelta
+        backend = "nccl" if torch.cuda.is_available() else "gloo"
+        if backend == "nccl":
+            torch.cuda.set_device(local)
+        dist.init_process_group(backend, timeout=timedelta(seconds=600))
+    return world, rank, local
+
+
+def dist_max(x: float, world: int) -> float:
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([x], dtype=torch.float64, device=dev)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def dist_barrier(world: int):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def reference_arm(args, world, rank):
+    """The reference's own CPU PDLP (solve_pdhg, src/pdlp.cpp:146, built from
+    its sources into oracle/_ref) on a bounded sample of the same LP."""
+    if rank != 0:
+        return None
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import b200pdlp as B
+    import oracle as O
+    if not O.reference_available():
+        return {"impl": "reference", "unavailable": "reference CPU engine not built (oracle/_ref/libsovref.so)"}
+    lp = make_lp(B, args.workload)
+    U, S, Dr, Dc, _ = B.prepare(lp)
+    sample = cpu_sample(O, U, args.cpu_sample_iters)
+    attempts = args.ref_attempts_per_solve
+    per_step = []
+    for _ in range(args.warmup + args.steps):
+        s = cpu_sample(O, U, args.cpu_sample_iters)
+        per_step.append(s["seconds"] / s["iterations"])
+    timed = per_step[args.warmup:]
+    sec_per_attempt = sum(timed) / len(timed)
+    value = 1.0 / (sec_per_attempt * attempts)
+    cb = {"value": value, "unit": UNIT, "cores": 1, "kind": "reference",
+          "sample": f"{args.cpu_sample_iters} attempts of solve_pdhg per step on this LP; solves/s = "
+                    f"attempts/s / {attempts} attempts per solve (the engine's count at 1e-6)"}
+    return {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1e3 * sec_per_attempt * args.cpu_sample_iters,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic", "impl": "reference", "config": workload_config(args, U, lp),
+            "cpu_baseline": cb, "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0,
+                                        "d2h_bytes_per_step": 0}, "sample_seconds": sample["seconds"]}
+
+
+_ref_problem_cache = {}
+
+
+def cpu_sample(O, U, iters):
+    key = id(U)
+    if key not in _ref_problem_cache:
+        _ref_problem_cache[key] = O.RefProblem.from_form(O.LPForm(U.m, U.n, U.row, U.col, U.val, U.c, U.rL, U.rU,
+                                                                  U.l, U.u, U.obj_offset), use_presolve=False)
+    P = _ref_problem_cache[key]
+    r = P.solve_pdhg(max_iterations=iters, check_every=64, tol=1e-6)
+    return {"seconds": r["seconds"], "iterations": r["iterations"]}
+
+
+def workload_config(args, U, lp):
+    return {"workload": describe(args.workload), "m": U.m, "n": U.n, "nnz": U.nnz, "tol": args.tol,
+            "check_every": 64, "precision": args.precision,
+            "l2": "inputs larger than L2 (working set > 126 MB)" if U.nnz * 16 > 126e6 else
+                  "inputs smaller than L2; no flush (every solve re-reads them)",
+            "parallelism": f"replicas x{args.gpus}" if args.gpus > 1 else "single GPU"}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="large", choices=sorted(WORKLOADS))
+    ap.add_argument("--tol", type=float, default=1e-6)
+    ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])
+    ap.add_argument("--e2e-steps", type=int, default=2)
+    ap.add_argument("--cpu-sample-iters", type=int, default=40)
+    ap.add_argument("--ref-attempts-per-solve", type=int, default=0,
+                    help="attempts per solve used to turn the reference's attempts/s into solves/s "
+                         "(0: take the engine's own count from a solve of this LP)")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    world, rank, local = dist_setup(args.gpus)
+
+    if args.impl == "reference":
+        if args.ref_attempts_per_solve <= 0:
+            args.ref_attempts_per_solve = 10_000
+        line = reference_arm(args, world, rank)
+        if rank == 0 and line is not None:
+            print(json.dumps(line), flush=True)
+        return
+
+    import torch
+    import b200pdlp as B
+    torch.cuda.set_device(local)
+    prec = B.PREC_MIXED if args.precision == "mixed" else B.PREC_FP64
+
+    t0 = time.time()
+    lp = make_lp(B, args.workload)
+    U, S, Dr, Dc, _ = B.prepare(lp)
+    t_prep = time.time() - t0
+    stream = torch.cuda.Stream()
+    opts = dict(precision=prec, stream=stream.cuda_stream)
+    eng = B.Engine(U, S, Dr, Dc, **opts)
+    info = eng.info()
+
+    def one_solve():
+        return eng.solve(max_iterations=2_000_000, check_every=64, tol=args.tol, copy_out=False, **opts)
+
+    for _ in range(args.warmup):
+        r = one_solve()
+    dist_barrier(world)
+    torch.cuda.synchronize()
+    results = []
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+    with ClockSampler(local) as clk:
+        ev[0].record(stream)
+        for _ in range(args.steps):
+            results.append(one_solve())
+        ev[1].record(stream)
+        torch.cuda.synchronize()
+    dist_barrier(world)
+    ms_total = ev[0].elapsed_time(ev[1])
+    ms_total = dist_max(ms_total, world)
+    value = world * args.steps / (ms_total / 1e3)
+    lat = sorted(r.stats["device_ms"] for r in results)
+
+    # roofline of the persistent kernel: algorithmic bytes of the accepted
+    # iterations (FP32 and FP64 phases) over the kernel's own CUDA-event time
+    peaks = {}
+    pp = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(pp):
+        peaks = json.load(open(pp))
+    peak_gbs = float(peaks.get("hbm_gbs", 6650.0))
+    peak_src = "measured" if "hbm_gbs" in peaks else "fallback"
+    m, n, z = U.m, U.n, U.nnz
+    tot_bytes, tot_ms = 0.0, 0.0
+    for r in results:
+        acc32 = r.stats["fp32_accepted"]
+        acc64 = r.stats["accepted"] - acc32
+        tot_bytes += acc32 * algorithmic_bytes(m, n, z, 4) + acc64 * algorithmic_bytes(m, n, z, 8)
+        tot_ms += r.stats["device_ms"]
+    achieved = tot_bytes / (tot_ms / 1e3) / 1e9
+
+    # standalone SpMV (A x, FP32), the kernel every pass is built on
+    spmv_ms = eng.spmv_bench(0, B.PREC_MIXED, 50, stream.cuda_stream)
+    spmv_t_ms = eng.spmv_bench(1, B.PREC_MIXED, 50, stream.cuda_stream)
+    spmv_gbs = spmv_bytes(m, n, z) / (spmv_ms / 1e3) / 1e9
+    spmv_t_gbs = spmv_bytes(n, m, z) / (spmv_t_ms / 1e3) / 1e9
+
+    # e2e: the drop-in C-ABI call with host buffers (layout build, H2D, solve, D2H)
+    e2e_ms = []
+    for i in range(args.e2e_steps + 1):
+        torch.cuda.synchronize()
+        t1 = time.perf_counter()
+        re = B.solve_pdhg_gpu(U, S, Dr, Dc, 0.99, 2_000_000, 64, args.tol, precision=prec)
+        e2e_ms.append((time.perf_counter() - t1) * 1e3)
+    e2e_ms = e2e_ms[1:]
+    e2e_max = dist_max(sum(e2e_ms), world)
+    e2e_value = world * len(e2e_ms) / (e2e_max / 1e3)
+    h2d = info["device_bytes"]
+    d2h = 8 * (m + n)
+
+    cpu = None
+    if rank == 0 and not args.no_cpu_baseline:
+        try:
+            sys.path.insert(0, os.path.join(ROOT, "oracle"))
+            import oracle as O
+            if O.reference_available():
+                s = cpu_sample(O, U, args.cpu_sample_iters)
+                attempts = statistics.median(r.iterations for r in results)
+                cpu = {"value": 1.0 / (s["seconds"] / s["iterations"] * attempts), "unit": UNIT, "cores": 1,
+                       "kind": "reference",
+                       "sample": f"{s['iterations']} attempts of the reference solve_pdhg ({s['seconds']:.2f} s) "
+                                 f"on this LP, extrapolated to {attempts} attempts per solve"}
+        except Exception as e:  # the baseline is reported, not required
+            cpu = {"error": str(e)}
+
+    if rank == 0:
+        clocks = clk.summary()
+        r0 = results[-1]
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_total / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64" if prec == B.PREC_MIXED else "f64",
+            "data": "synthetic", "config": workload_config(args, U, lp),
+            "latency_ms": {"p50": lat[len(lat) // 2], "p99": lat[min(len(lat) - 1, int(0.99 * len(lat)))],
+                           "max": lat[-1]},
+            "solve": {"attempts": r0.iterations, "accepted": r0.stats["accepted"],
+                      "fp32_attempts": r0.stats["fp32_attempts"], "restarts": r0.restarts,
+                      "checks": r0.stats["checks"], "eps": [r0.eps_P, r0.eps_D, r0.eps_G],
+                      "converged": r0.converged, "attempts_per_s": r0.iterations / (r0.stats["device_ms"] / 1e3)},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak_gbs, "unit": "GB/s",
+                         "frac": achieved / peak_gbs, "traffic": None,
+                         "kernel": "k_pdlp (persistent solve)", "peak_source": peak_src},
+            "spmv": {"A_gbs": spmv_gbs, "AT_gbs": spmv_t_gbs, "A_ms": spmv_ms, "AT_ms": spmv_t_ms,
+                     "frac_A": spmv_gbs / peak_gbs, "frac_AT": spmv_t_gbs / peak_gbs},
+            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                    "ms_per_step": statistics.mean(e2e_ms)},
+            "cpu_baseline": cpu, "clocks": clocks, "gpu_launches": sum(
+                1 + (1 if r.stats["fp32_attempts"] and r.stats["fp32_attempts"] < r.iterations else 0)
+                for r in results),
+            "prep_s": t_prep, "layout": {k: info[k] for k in ("ctas", "a_padded", "at_padded", "values_exact_fp32")},
+        }
+        print(json.dumps(line), flush=True)
+    eng.close()
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,181 @@
+/* b200_pdlp.h -- C ABI of the B200 PDLP engine (libb200pdlp.so).
+ *
+ * The engine replaces the reference solver's CUDA backend behind its GPU
+ * entry point
+ *
+ *     PdlpResult solve_pdhg_gpu(const RangedLP& unscaled_form, const RangedLP& scaled_form,
+ *                               const std::vector<double>& Dr, const std::vector<double>& Dc,
+ *                               double eta, int max_iterations, int check_every, double tol,
+ *                               std::atomic<bool>* stop_flag);
+ *     (include/pdlp_gpu.hpp:22-25, implemented by gpu/pdlp_gpu_solve.cu:261-267)
+ *
+ * Everything here is plain C: pointers, sizes and int status codes; no C++
+ * types and no exceptions cross it. The C++ shim that gives the reference
+ * its exact solve_pdhg_gpu symbol is team-suprema_b200/csrc/shim_solve_pdhg_gpu.cpp.
+ *
+ * Threading: every entry point is thread-safe for distinct engines; one
+ * engine must not be used by two threads at once. Errors: a non-zero return
+ * is one of the B2_ERR_* codes and b2_last_error() (thread-local) says why.
+ */
+#ifndef B200_PDLP_H
+#define B200_PDLP_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ---------------------------------------------------- */
+#define B2_OK 0
+#define B2_ERR_INVALID 1     /* malformed input (indices, sizes, non-PDLP form)        */
+#define B2_ERR_CUDA 2        /* CUDA runtime error                                       */
+#define B2_ERR_OOM 3         /* device allocation failed                                 */
+#define B2_ERR_TIMEOUT 4     /* a device-side barrier wait ran out of time (kernel exits) */
+#define B2_ERR_NO_DEVICE 5   /* no CUDA device                                           */
+#define B2_ERR_NONFINITE 6   /* NaN / inf where a finite number is required              */
+#define B2_ERR_UNSUPPORTED 7 /* request outside what this build supports                 */
+
+/* ---- one LP, as the reference's RangedLP holds it ---------------------
+ * rL <= A x <= rU, l <= x <= u, minimise c'x + obj_offset; A in COO
+ * (SparseMatrix, include/sparse.hpp:14-22; RangedLP, include/ranged_lp.hpp:10-27). */
+typedef struct b2_lp_view {
+    int32_t m, n;
+    int64_t nnz;
+    const int32_t* row_idx;
+    const int32_t* col_idx;
+    const double* val;
+    const double* c;
+    const double* rL;
+    const double* rU;
+    const double* l;
+    const double* u;
+    double obj_offset;
+} b2_lp_view;
+
+/* ---- solve options ---------------------------------------------------- */
+#define B2_PREC_FP64 0   /* FP64 iterates and accumulation throughout                       */
+#define B2_PREC_MIXED 1  /* FP32 iterates / SpMV first, then FP64 iterates to `tol` (default) */
+
+typedef struct b2_solve_opts {
+    int32_t max_iterations;   /* attempts, counted as include/pdlp_algo.hpp:103-108      */
+    int32_t check_every;      /* accepted steps between KKT checks (callers pass 64)      */
+    double tol;               /* max(eps_P, eps_D, eps_G) on the unscaled PDLP form       */
+    int32_t precision;        /* B2_PREC_*                                                 */
+    double switch_tol;        /* MIXED: KKT level at which FP32 iterates hand over to FP64 */
+    int32_t stall_checks;     /* MIXED: checks without a new best point before handing over */
+    double time_limit_s;      /* <= 0: none. Device-side wall clock; exits like stop_flag  */
+    double barrier_timeout_s; /* <= 0: 10 s. Bound on every device-side wait               */
+    int32_t max_ctas;         /* <= 0: auto (co-resident CTAs of the persistent kernel)     */
+    int32_t lane_target;      /* <= 0: auto. Entries per lane that picks lanes-per-row      */
+    int32_t sigma_window;     /* <= 0: auto. Rows per sigma-sort window of the sliced format */
+    int32_t return_current;   /* debug: return the current iterate, not the chosen/best    */
+    void* stream;             /* cudaStream_t to launch on; NULL: the engine's own stream  */
+    int32_t debug_delay_us;   /* test hook: CTA 0 reaches its first barrier this late (bounded),
+                                 so a short barrier_timeout_s exercises the timeout path   */
+} b2_solve_opts;
+
+void b2_default_opts(b2_solve_opts* opts);
+
+/* ---- result ------------------------------------------------------------
+ * Mirrors PdlpResult (include/pdlp.hpp:18-24) plus engine counters. x/y are
+ * written to caller buffers in unscaled PDLP-form space (x = Dc*x_s, y = Dr*y_s). */
+#define B2_EXIT_CONVERGED 1
+#define B2_EXIT_MAX_ITER 2
+#define B2_EXIT_STOPPED 3
+#define B2_EXIT_TIME_LIMIT 4
+
+typedef struct b2_result {
+    int32_t iterations;    /* attempts, as PdlpResult::iterations */
+    int32_t restarts;
+    int32_t converged;
+    int32_t accepted;      /* accepted PDHG steps                  */
+    double eps_P, eps_D, eps_G;
+    double objective;      /* c'x + obj_offset of the returned point (PDLP form) */
+    int32_t exit_reason;   /* B2_EXIT_*                            */
+    int32_t checks;        /* KKT checks performed on the device   */
+    int32_t fp32_attempts; /* attempts run with FP32 iterates      */
+    int32_t fp32_accepted;
+    double device_ms;      /* persistent-kernel time (CUDA events)  */
+    double host_ms;        /* whole call, host clock                */
+    double final_eta, final_omega;
+} b2_result;
+
+/* Drop-in for solve_pdhg_gpu (include/pdlp_gpu.hpp:22-25): same inputs in the
+ * same order, `eta` ignored (adaptive, as gpu/pdlp_gpu_solve.cu:263), stop_flag
+ * polled by the device about every 16 attempts (may be NULL). x_out (n) and
+ * y_out (m) receive the returned point. Uses the default options above. */
+int b2_solve_pdhg_gpu(const b2_lp_view* unscaled_form, const b2_lp_view* scaled_form, const double* Dr,
+                      const double* Dc, double eta, int32_t max_iterations, int32_t check_every, double tol,
+                      const volatile int32_t* stop_flag, double* x_out, double* y_out, b2_result* res);
+
+/* Same, with explicit options (max_iterations / check_every / tol taken from opts). */
+int b2_solve_pdhg_gpu_ex(const b2_lp_view* unscaled_form, const b2_lp_view* scaled_form, const double* Dr,
+                         const double* Dc, const b2_solve_opts* opts, const volatile int32_t* stop_flag,
+                         double* x_out, double* y_out, b2_result* res);
+
+/* ---- resident engine: upload once, solve many times ---------------------
+ * b2_engine_create does what the reference's GpuBackend constructor does
+ * (gpu/pdlp_gpu_solve.cu:198-205): builds the device layout of A and A^T and
+ * uploads the problem. b2_engine_solve then runs from HBM-resident data. */
+typedef struct b2_engine b2_engine;
+
+int b2_engine_create(const b2_lp_view* unscaled_form, const b2_lp_view* scaled_form, const double* Dr,
+                     const double* Dc, const b2_solve_opts* opts, b2_engine** out);
+int b2_engine_solve(b2_engine* e, const b2_solve_opts* opts, const volatile int32_t* stop_flag, double* x_out,
+                    double* y_out, b2_result* res);
+void b2_engine_destroy(b2_engine* e);
+
+typedef struct b2_engine_info {
+    int32_t m, n;
+    int64_t nnz;
+    int64_t a_slices, at_slices;
+    int64_t a_padded, at_padded;   /* stored entries incl. padding */
+    int32_t values_exact_fp32;     /* 1: A's values are exact in FP32 (no FP64 copy kept) */
+    int32_t ctas, threads_per_cta; /* persistent-kernel launch shape */
+    int32_t sm_count;
+    int64_t device_bytes;          /* HBM held by the engine */
+} b2_engine_info;
+int b2_engine_get_info(b2_engine* e, b2_engine_info* info);
+
+/* y = A x (which = 0) or y = A^T x (which = 1) through the engine's device
+ * SpMV (stored values, FP64 accumulation); x and y in the caller's order. */
+int b2_engine_spmv(b2_engine* e, int32_t which, const double* x, double* y);
+
+/* Times `reps` launches of the standalone SpMV kernel on resident data with
+ * CUDA events on `stream` (NULL: the engine's stream). precision: B2_PREC_MIXED
+ * times FP32 x/y, B2_PREC_FP64 times FP64 x/y (FP32 values either way when
+ * they are exact). avg_ms receives the mean time per launch. */
+int b2_engine_spmv_bench(b2_engine* e, int32_t which, int32_t precision, int32_t reps, void* stream,
+                         double* avg_ms);
+
+/* ---- host-side preparation (product side, no GPU needed) ---------------- */
+
+/* Ruiz (ruiz_passes) + Pock-Chambolle alpha=1 scaling, as scale() in
+ * src/scaling.cpp:25-84 (LP case). Outputs in caller buffers: scaled values in
+ * COO order (nnz), c/l/u (n), rL/rU (m), Dr (m), Dc (n). */
+int b2_scale(const b2_lp_view* lp, int32_t ruiz_passes, double* val_s, double* c_s, double* rL_s, double* rU_s,
+             double* l_s, double* u_s, double* Dr, double* Dc);
+
+/* Synthetic LPs of the benchmark shapes (seeded, deterministic):
+ * equality-form LP min c'x, Ax = b, 0 <= x <= 10, `k` distinct uniform rows per
+ * column with values U[-1,1] (rounded to FP32 when fp32_values), x0 ~ U[0,5],
+ * b = A x0, y0 ~ N(0,1), z0 ~ U[0,1], c = A'y0 + z0. Buffers: row/col/val
+ * (n*k), c/l/u (n), rL/rU (m). */
+int b2_gen_random_lp(int32_t m, int32_t n, int32_t k, uint64_t seed, int32_t fp32_values, int32_t* row,
+                     int32_t* col, double* val, double* c, double* rL, double* rU, double* l, double* u);
+
+/* Balanced transportation LP: S sources x D sinks, n = S*D arcs, m = S + D
+ * equality rows, 2 unit entries per column; supplies integer U[100,1000],
+ * demands an integer partition of the total, costs integer U[1,100],
+ * 0 <= x < inf. Buffers: row/col/val (2n), c/l/u (n), rL/rU (m). */
+int b2_gen_transport(int32_t S, int32_t D, uint64_t seed, int32_t* row, int32_t* col, double* val, double* c,
+                     double* rL, double* rU, double* l, double* u);
+
+const char* b2_last_error(void);
+const char* b2_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* B200_PDLP_H */

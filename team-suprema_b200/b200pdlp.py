@@ -1,0 +1,399 @@
+"""B200 PDLP engine -- Python mirror of the reference solver's GPU PDLP entry point.
+
+The product is ``libb200pdlp.so`` (CUDA sm_100a kernels + C++ host side + the C
+ABI declared in ``include/b200_pdlp.h``). This module binds that ABI with
+ctypes and mirrors the reference interface it replaces:
+
+* ``solve_pdhg_gpu(unscaled_form, scaled_form, Dr, Dc, eta, max_iterations,
+  check_every, tol, stop_flag)`` -> ``PdlpResult``: the same arguments, in the same
+  order and with the same meaning, as ``solve_pdhg_gpu`` in the reference's
+  include/pdlp_gpu.hpp:22-25; ``PdlpResult`` has the fields of
+  include/pdlp.hpp:18-24. Errors raise ``RuntimeError`` (the reference throws
+  ``std::runtime_error``, gpu/pdlp_gpu_solve.cu:32-38); a non-converged solve is
+  a normal result with ``converged = False``.
+* ``RangedLP`` holds an LP as include/ranged_lp.hpp:10-27 does (COO matrix).
+* ``Engine`` keeps a problem resident on the GPU for repeated solves.
+
+There is no CPU fallback: importing works without a GPU, but every solve
+needs the CUDA library and a device, and fails loudly otherwise.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import threading
+from dataclasses import dataclass, field
+from typing import Optional
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libb200pdlp.so")
+INCLUDE_H = os.path.join(os.path.dirname(HERE), "include", "b200_pdlp.h")
+
+B2_OK, B2_ERR_INVALID, B2_ERR_CUDA, B2_ERR_OOM, B2_ERR_TIMEOUT, B2_ERR_NO_DEVICE, B2_ERR_NONFINITE, \
+    B2_ERR_UNSUPPORTED = range(8)
+PREC_FP64, PREC_MIXED = 0, 1
+EXIT_CONVERGED, EXIT_MAX_ITER, EXIT_STOPPED, EXIT_TIME_LIMIT = 1, 2, 3, 4
+
+EXPORTED = [
+    "b2_default_opts", "b2_solve_pdhg_gpu", "b2_solve_pdhg_gpu_ex", "b2_engine_create", "b2_engine_solve",
+    "b2_engine_destroy", "b2_engine_get_info", "b2_engine_spmv", "b2_engine_spmv_bench", "b2_scale",
+    "b2_gen_random_lp", "b2_gen_transport", "b2_last_error", "b2_version",
+]
+
+
+class B2Error(RuntimeError):
+    """A non-zero B2_ERR_* status from the C ABI."""
+
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"b200 pdlp error {code}: {msg}")
+        self.code = code
+
+
+class _LPView(C.Structure):
+    _fields_ = [("m", C.c_int32), ("n", C.c_int32), ("nnz", C.c_int64),
+                ("row_idx", C.c_void_p), ("col_idx", C.c_void_p), ("val", C.c_void_p),
+                ("c", C.c_void_p), ("rL", C.c_void_p), ("rU", C.c_void_p),
+                ("l", C.c_void_p), ("u", C.c_void_p), ("obj_offset", C.c_double)]
+
+
+class SolveOpts(C.Structure):
+    _fields_ = [("max_iterations", C.c_int32), ("check_every", C.c_int32), ("tol", C.c_double),
+                ("precision", C.c_int32), ("switch_tol", C.c_double), ("stall_checks", C.c_int32),
+                ("time_limit_s", C.c_double), ("barrier_timeout_s", C.c_double), ("max_ctas", C.c_int32),
+                ("lane_target", C.c_int32), ("sigma_window", C.c_int32), ("return_current", C.c_int32),
+                ("stream", C.c_void_p), ("debug_delay_us", C.c_int32)]
+
+
+class _Result(C.Structure):
+    _fields_ = [("iterations", C.c_int32), ("restarts", C.c_int32), ("converged", C.c_int32),
+                ("accepted", C.c_int32), ("eps_P", C.c_double), ("eps_D", C.c_double), ("eps_G", C.c_double),
+                ("objective", C.c_double), ("exit_reason", C.c_int32), ("checks", C.c_int32),
+                ("fp32_attempts", C.c_int32), ("fp32_accepted", C.c_int32), ("device_ms", C.c_double),
+                ("host_ms", C.c_double), ("final_eta", C.c_double), ("final_omega", C.c_double)]
+
+
+class EngineInfo(C.Structure):
+    _fields_ = [("m", C.c_int32), ("n", C.c_int32), ("nnz", C.c_int64), ("a_slices", C.c_int64),
+                ("at_slices", C.c_int64), ("a_padded", C.c_int64), ("at_padded", C.c_int64),
+                ("values_exact_fp32", C.c_int32), ("ctas", C.c_int32), ("threads_per_cta", C.c_int32),
+                ("sm_count", C.c_int32), ("device_bytes", C.c_int64)]
+
+
+_lib = None
+_lib_lock = threading.Lock()
+
+
+def lib():
+    """The loaded CUDA library; raises if it has not been built."""
+    global _lib
+    with _lib_lock:
+        if _lib is None:
+            if not os.path.exists(LIB_PATH):
+                raise RuntimeError(f"libb200pdlp.so is not built ({LIB_PATH}); run __graft_entry__.build()")
+            L = C.CDLL(LIB_PATH)
+            vp, i32, i64, f64 = C.c_void_p, C.c_int32, C.c_int64, C.c_double
+            L.b2_last_error.restype = C.c_char_p
+            L.b2_version.restype = C.c_char_p
+            L.b2_default_opts.argtypes = [C.POINTER(SolveOpts)]
+            L.b2_solve_pdhg_gpu.argtypes = [C.POINTER(_LPView), C.POINTER(_LPView), vp, vp, f64, i32, i32, f64,
+                                            vp, vp, vp, C.POINTER(_Result)]
+            L.b2_solve_pdhg_gpu_ex.argtypes = [C.POINTER(_LPView), C.POINTER(_LPView), vp, vp,
+                                               C.POINTER(SolveOpts), vp, vp, vp, C.POINTER(_Result)]
+            L.b2_engine_create.argtypes = [C.POINTER(_LPView), C.POINTER(_LPView), vp, vp, C.POINTER(SolveOpts),
+                                           C.POINTER(vp)]
+            L.b2_engine_solve.argtypes = [vp, C.POINTER(SolveOpts), vp, vp, vp, C.POINTER(_Result)]
+            L.b2_engine_destroy.argtypes = [vp]
+            L.b2_engine_destroy.restype = None
+            L.b2_engine_get_info.argtypes = [vp, C.POINTER(EngineInfo)]
+            L.b2_engine_spmv.argtypes = [vp, i32, vp, vp]
+            L.b2_engine_spmv_bench.argtypes = [vp, i32, i32, i32, vp, C.POINTER(f64)]
+            L.b2_scale.argtypes = [C.POINTER(_LPView), i32] + [vp] * 8
+            L.b2_gen_random_lp.argtypes = [i32, i32, i32, C.c_uint64, i32] + [vp] * 8
+            L.b2_gen_transport.argtypes = [i32, i32, C.c_uint64] + [vp] * 8
+            _lib = L
+        return _lib
+
+
+def _check(rc: int):
+    if rc != B2_OK:
+        raise B2Error(rc, lib().b2_last_error().decode())
+
+
+def _ptr(a: Optional[np.ndarray]):
+    return None if a is None else a.ctypes.data
+
+
+@dataclass
+class RangedLP:
+    """rL <= A x <= rU, l <= x <= u, min c'x + obj_offset (include/ranged_lp.hpp:10-27), A in COO."""
+
+    m: int
+    n: int
+    row: np.ndarray
+    col: np.ndarray
+    val: np.ndarray
+    c: np.ndarray
+    rL: np.ndarray
+    rU: np.ndarray
+    l: np.ndarray
+    u: np.ndarray
+    obj_offset: float = 0.0
+
+    def __post_init__(self):
+        self.m, self.n = int(self.m), int(self.n)
+        self.row = np.ascontiguousarray(self.row, np.int32)
+        self.col = np.ascontiguousarray(self.col, np.int32)
+        for k in ("val", "c", "rL", "rU", "l", "u"):
+            setattr(self, k, np.ascontiguousarray(getattr(self, k), np.float64))
+        self.obj_offset = float(self.obj_offset)
+
+    @property
+    def nnz(self) -> int:
+        return int(self.val.size)
+
+    @classmethod
+    def like(cls, other) -> "RangedLP":
+        """Copy of any object with the same fields (e.g. the oracle's LPForm)."""
+        return cls(other.m, other.n, other.row, other.col, other.val, other.c, other.rL, other.rU, other.l,
+                   other.u, getattr(other, "obj_offset", 0.0))
+
+    def view(self) -> _LPView:
+        return _LPView(self.m, self.n, self.nnz, _ptr(self.row), _ptr(self.col), _ptr(self.val), _ptr(self.c),
+                       _ptr(self.rL), _ptr(self.rU), _ptr(self.l), _ptr(self.u), self.obj_offset)
+
+
+@dataclass
+class PdlpResult:
+    """Fields of the reference's PdlpResult (include/pdlp.hpp:18-24) plus engine counters."""
+
+    x: np.ndarray
+    y: np.ndarray
+    iterations: int = 0
+    converged: bool = False
+    eps_P: float = 0.0
+    eps_D: float = 0.0
+    eps_G: float = 0.0
+    restarts: int = 0
+    stats: dict = field(default_factory=dict)
+
+
+class StopFlag:
+    """Cooperative cancellation word, the counterpart of std::atomic<bool>* stop_flag
+    (include/pdlp.hpp:30-34): set() from any thread; the device polls it."""
+
+    def __init__(self):
+        self._v = C.c_int32(0)
+
+    def set(self):
+        self._v.value = 1
+
+    def clear(self):
+        self._v.value = 0
+
+    def is_set(self) -> bool:
+        return bool(self._v.value)
+
+    @property
+    def ptr(self):
+        return C.addressof(self._v)
+
+
+def default_opts(**kw) -> SolveOpts:
+    o = SolveOpts()
+    lib().b2_default_opts(C.byref(o))
+    for k, v in kw.items():
+        if not hasattr(o, k):
+            raise TypeError(f"unknown option {k}")
+        setattr(o, k, v)
+    return o
+
+
+def _result(r: _Result, x, y) -> PdlpResult:
+    stats = {k: getattr(r, k) for k, _ in _Result._fields_}
+    return PdlpResult(x=x, y=y, iterations=r.iterations, converged=bool(r.converged), eps_P=r.eps_P,
+                      eps_D=r.eps_D, eps_G=r.eps_G, restarts=r.restarts, stats=stats)
+
+
+def _vec(a, n) -> np.ndarray:
+    a = np.ascontiguousarray(a, np.float64)
+    if a.size != n:
+        raise ValueError(f"expected {n} values, got {a.size}")
+    return a
+
+
+def solve_pdhg_gpu(unscaled_form: RangedLP, scaled_form: RangedLP, Dr, Dc, eta: float = 0.99,
+                   max_iterations: int = 200000, check_every: int = 64, tol: float = 1e-6,
+                   stop_flag: Optional[StopFlag] = None, **opts) -> PdlpResult:
+    """Drop-in for the reference's solve_pdhg_gpu (include/pdlp_gpu.hpp:22-25).
+
+    unscaled_form is the PDLP form (build_pdlp_form), scaled_form = scale(unscaled_form)
+    with scalings Dr, Dc. `eta` is ignored: the step size is adaptive, as in the
+    reference (gpu/pdlp_gpu_solve.cu:263). Extra keyword options map to
+    ``b2_solve_opts`` (precision, switch_tol, time_limit_s, ...).
+    """
+    U = RangedLP.like(unscaled_form)
+    S = RangedLP.like(scaled_form)
+    Dr = _vec(Dr, U.m)
+    Dc = _vec(Dc, U.n)
+    o = default_opts(max_iterations=int(max_iterations), check_every=int(check_every), tol=float(tol), **opts)
+    x = np.zeros(max(U.n, 1))
+    y = np.zeros(max(U.m, 1))
+    r = _Result()
+    uv, sv = U.view(), S.view()
+    _check(lib().b2_solve_pdhg_gpu_ex(C.byref(uv), C.byref(sv), _ptr(Dr), _ptr(Dc), C.byref(o),
+                                      stop_flag.ptr if stop_flag else None, _ptr(x), _ptr(y), C.byref(r)))
+    return _result(r, x[:U.n], y[:U.m])
+
+
+class Engine:
+    """A PDLP problem resident in HBM (b2_engine_*): create once, solve many times."""
+
+    def __init__(self, unscaled_form: RangedLP, scaled_form: RangedLP, Dr, Dc, **opts):
+        self.U = RangedLP.like(unscaled_form)
+        S = RangedLP.like(scaled_form)
+        Dr = _vec(Dr, self.U.m)
+        Dc = _vec(Dc, self.U.n)
+        o = default_opts(**opts)
+        h = C.c_void_p()
+        uv, sv = self.U.view(), S.view()
+        _check(lib().b2_engine_create(C.byref(uv), C.byref(sv), _ptr(Dr), _ptr(Dc), C.byref(o), C.byref(h)))
+        self._h = h
+
+    def close(self):
+        if getattr(self, "_h", None) and self._h.value:
+            lib().b2_engine_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def solve(self, max_iterations: int = 200000, check_every: int = 64, tol: float = 1e-6,
+              stop_flag: Optional[StopFlag] = None, copy_out: bool = True, **opts) -> PdlpResult:
+        o = default_opts(max_iterations=int(max_iterations), check_every=int(check_every), tol=float(tol), **opts)
+        x = np.zeros(max(self.U.n, 1)) if copy_out else None
+        y = np.zeros(max(self.U.m, 1)) if copy_out else None
+        r = _Result()
+        _check(lib().b2_engine_solve(self._h, C.byref(o), stop_flag.ptr if stop_flag else None, _ptr(x), _ptr(y),
+                                     C.byref(r)))
+        return _result(r, None if x is None else x[:self.U.n], None if y is None else y[:self.U.m])
+
+    def info(self) -> dict:
+        i = EngineInfo()
+        _check(lib().b2_engine_get_info(self._h, C.byref(i)))
+        return {k: getattr(i, k) for k, _ in EngineInfo._fields_}
+
+    def spmv(self, which: int, x) -> np.ndarray:
+        """A x (which=0) or A^T x (which=1) through the device SpMV (FP64 accumulation)."""
+        rows, cols = (self.U.m, self.U.n) if which == 0 else (self.U.n, self.U.m)
+        xx = _vec(x, cols)
+        if xx.size == 0:
+            xx = np.zeros(1)
+        y = np.zeros(max(rows, 1))
+        _check(lib().b2_engine_spmv(self._h, which, _ptr(xx), _ptr(y)))
+        return y[:rows]
+
+    def spmv_bench(self, which: int, precision: int = PREC_MIXED, reps: int = 20, stream=None) -> float:
+        ms = C.c_double()
+        _check(lib().b2_engine_spmv_bench(self._h, which, precision, reps, stream, C.byref(ms)))
+        return ms.value
+
+
+# ------------------------------------------------------------- host-side prep
+def scale(lp: RangedLP, ruiz_passes: int = 10):
+    """Ruiz + Pock-Chambolle scaling (src/scaling.cpp:25-84). Returns (scaled, Dr, Dc)."""
+    lp = RangedLP.like(lp)
+    vs = np.zeros(max(lp.nnz, 1)); cs = np.zeros(max(lp.n, 1)); rls = np.zeros(max(lp.m, 1))
+    rus = np.zeros(max(lp.m, 1)); ls = np.zeros(max(lp.n, 1)); us = np.zeros(max(lp.n, 1))
+    Dr = np.zeros(max(lp.m, 1)); Dc = np.zeros(max(lp.n, 1))
+    v = lp.view()
+    _check(lib().b2_scale(C.byref(v), ruiz_passes, *[_ptr(a) for a in (vs, cs, rls, rus, ls, us, Dr, Dc)]))
+    s = RangedLP(lp.m, lp.n, lp.row, lp.col, vs[:lp.nnz], cs[:lp.n], rls[:lp.m], rus[:lp.m], ls[:lp.n],
+                 us[:lp.n], lp.obj_offset)
+    return s, Dr[:lp.m], Dc[:lp.n]
+
+
+def build_pdlp_form(lp: RangedLP):
+    """PDLP form of a ranged LP, as build_pdlp_form (src/pdlp.cpp:8-82): equality rows
+    first, then one-sided rows as A x >= b (<= rows negated), ranged rows become an
+    equality with a bounded slack column, free rows are dropped. Returns
+    (form, meta) with meta = (row_perm, row_signs, n_orig, m_orig)."""
+    lp = RangedLP.like(lp)
+    rL, rU = lp.rL, lp.rU
+    eq = [], []
+    ineq = [], [], []
+    slack = []
+    slack_of = {}
+    for i in range(lp.m):
+        lo, hi = rL[i], rU[i]
+        if lo == hi:
+            eq[0].append(i); eq[1].append(lo)
+        elif np.isfinite(lo) and np.isfinite(hi):
+            slack_of[i] = len(slack); slack.append((lo, hi))
+            eq[0].append(i); eq[1].append(0.0)
+        elif np.isfinite(hi):
+            ineq[0].append(i); ineq[1].append(-1.0); ineq[2].append(-hi)
+        elif np.isfinite(lo):
+            ineq[0].append(i); ineq[1].append(1.0); ineq[2].append(lo)
+    row_perm = np.array(eq[0] + ineq[0], np.int64)
+    signs = np.array([1.0] * len(eq[0]) + ineq[1])
+    pos = np.full(lp.m, -1, np.int64)
+    pos[row_perm] = np.arange(row_perm.size)
+    p = pos[lp.row]
+    keep = p >= 0
+    rows = [p[keep]]
+    cols = [lp.col[keep]]
+    vals = [lp.val[keep] * signs[p[keep]]]
+    n2 = lp.n + len(slack)
+    for k, i in enumerate(eq[0]):
+        if i in slack_of:
+            rows.append(np.array([k])); cols.append(np.array([lp.n + slack_of[i]])); vals.append(np.array([-1.0]))
+    b = np.array(eq[1] + ineq[2], np.float64)
+    rU2 = np.concatenate([np.array(eq[1], np.float64), np.full(len(ineq[0]), np.inf)])
+    l2 = np.concatenate([lp.l, np.array([s[0] for s in slack], np.float64)])
+    u2 = np.concatenate([lp.u, np.array([s[1] for s in slack], np.float64)])
+    c2 = np.concatenate([lp.c, np.zeros(len(slack))])
+    form = RangedLP(row_perm.size, n2, np.concatenate(rows), np.concatenate(cols), np.concatenate(vals), c2, b,
+                    rU2, l2, u2, lp.obj_offset)
+    return form, (row_perm, signs, lp.n, lp.m)
+
+
+def gen_random_lp(m: int, n: int, k: int, seed: int = 0, fp32_values: bool = False) -> RangedLP:
+    """Equality-form random LP of the benchmark family (see include/b200_pdlp.h)."""
+    z = n * k
+    row = np.zeros(z, np.int32); col = np.zeros(z, np.int32); val = np.zeros(z)
+    c = np.zeros(n); rL = np.zeros(m); rU = np.zeros(m); l = np.zeros(n); u = np.zeros(n)
+    _check(lib().b2_gen_random_lp(m, n, k, seed, int(fp32_values), *[_ptr(a) for a in (row, col, val, c, rL, rU,
+                                                                                       l, u)]))
+    return RangedLP(m, n, row, col, val, c, rL, rU, l, u)
+
+
+def gen_transport(S: int, D: int, seed: int = 0) -> RangedLP:
+    """Balanced transportation LP of the benchmark family (see include/b200_pdlp.h)."""
+    n, m = S * D, S + D
+    row = np.zeros(2 * n, np.int32); col = np.zeros(2 * n, np.int32); val = np.zeros(2 * n)
+    c = np.zeros(n); rL = np.zeros(m); rU = np.zeros(m); l = np.zeros(n); u = np.zeros(n)
+    _check(lib().b2_gen_transport(S, D, seed, *[_ptr(a) for a in (row, col, val, c, rL, rU, l, u)]))
+    return RangedLP(m, n, row, col, val, c, rL, rU, l, u)
+
+
+def prepare(lp: RangedLP):
+    """Host pipeline up to the engine's inputs for an LP without presolve:
+    build_pdlp_form -> scale. Returns (unscaled_form, scaled_form, Dr, Dc, meta)."""
+    form, meta = build_pdlp_form(lp)
+    scaled, Dr, Dc = scale(form)
+    return form, scaled, Dr, Dc, meta
+
+
+def version() -> str:
+    return lib().b2_version().decode()

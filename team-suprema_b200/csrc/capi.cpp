@@ -1,0 +1,164 @@
+// capi.cpp -- the extern "C" boundary of libb200pdlp.so (include/b200_pdlp.h).
+// Every entry point converts internal errors into a B2_ERR_* status plus a
+// thread-local message; no exception crosses the ABI.
+#include <chrono>
+#include <cstring>
+#include <exception>
+#include <new>
+#include <string>
+
+#include "b200_pdlp.h"
+#include "internal.h"
+
+namespace b2 {
+
+namespace {
+thread_local std::string g_last_error;
+}
+
+void set_last_error(const std::string& msg) { g_last_error = msg; }
+
+[[noreturn]] void fail(int code, const std::string& msg) { throw Error{code, msg}; }
+
+template <class F>
+int guarded(F&& f) {
+    try {
+        f();
+        g_last_error.clear();
+        return B2_OK;
+    } catch (const Error& e) {
+        g_last_error = e.msg;
+        return e.code;
+    } catch (const std::bad_alloc&) {
+        g_last_error = "host allocation failed";
+        return B2_ERR_OOM;
+    } catch (const std::exception& e) {
+        g_last_error = e.what();
+        return B2_ERR_INVALID;
+    } catch (...) {
+        g_last_error = "unknown error";
+        return B2_ERR_INVALID;
+    }
+}
+
+}  // namespace b2
+
+struct b2_engine {
+    b2::EngineImpl* impl;
+};
+
+extern "C" {
+
+void b2_default_opts(b2_solve_opts* o) {
+    std::memset(o, 0, sizeof(*o));
+    o->max_iterations = 200000;   // solve_pdhg default (include/pdlp.hpp:35-38)
+    o->check_every = 64;
+    o->tol = 1e-6;
+    o->precision = B2_PREC_MIXED;
+    o->switch_tol = 1e-5;
+    o->stall_checks = 8;
+    o->time_limit_s = 0.0;
+    o->barrier_timeout_s = 10.0;
+}
+
+const char* b2_last_error(void) { return b2::g_last_error.c_str(); }
+
+const char* b2_version(void) { return "b200-pdlp 0.1 (sm_100a)"; }
+
+int b2_solve_pdhg_gpu_ex(const b2_lp_view* U, const b2_lp_view* S, const double* Dr, const double* Dc,
+                         const b2_solve_opts* opts, const volatile int32_t* stop_flag, double* x_out, double* y_out,
+                         b2_result* res) {
+    return b2::guarded([&] {
+        if (!U || !S || !opts) b2::fail(B2_ERR_INVALID, "null argument");
+        const auto t0 = std::chrono::steady_clock::now();
+        b2::EngineImpl* e = b2::engine_create(*U, *S, Dr, Dc, *opts);
+        try {
+            b2::engine_solve(e, *opts, stop_flag, x_out, y_out, res);
+        } catch (...) {
+            b2::engine_destroy(e);
+            throw;
+        }
+        b2::engine_destroy(e);
+        if (res) res->host_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+    });
+}
+
+int b2_solve_pdhg_gpu(const b2_lp_view* U, const b2_lp_view* S, const double* Dr, const double* Dc, double /*eta*/,
+                      int32_t max_iterations, int32_t check_every, double tol, const volatile int32_t* stop_flag,
+                      double* x_out, double* y_out, b2_result* res) {
+    b2_solve_opts o;
+    b2_default_opts(&o);
+    o.max_iterations = max_iterations;
+    o.check_every = check_every;
+    o.tol = tol;
+    return b2_solve_pdhg_gpu_ex(U, S, Dr, Dc, &o, stop_flag, x_out, y_out, res);
+}
+
+int b2_engine_create(const b2_lp_view* U, const b2_lp_view* S, const double* Dr, const double* Dc,
+                     const b2_solve_opts* opts, b2_engine** out) {
+    return b2::guarded([&] {
+        if (!U || !S || !out) b2::fail(B2_ERR_INVALID, "null argument");
+        b2_solve_opts o;
+        if (opts) o = *opts;
+        else b2_default_opts(&o);
+        *out = nullptr;
+        b2::EngineImpl* e = b2::engine_create(*U, *S, Dr, Dc, o);
+        *out = new b2_engine{e};
+    });
+}
+
+int b2_engine_solve(b2_engine* e, const b2_solve_opts* opts, const volatile int32_t* stop_flag, double* x_out,
+                    double* y_out, b2_result* res) {
+    return b2::guarded([&] {
+        if (!e || !opts) b2::fail(B2_ERR_INVALID, "null argument");
+        b2::engine_solve(e->impl, *opts, stop_flag, x_out, y_out, res);
+    });
+}
+
+void b2_engine_destroy(b2_engine* e) {
+    if (!e) return;
+    b2::engine_destroy(e->impl);
+    delete e;
+}
+
+int b2_engine_get_info(b2_engine* e, b2_engine_info* info) {
+    return b2::guarded([&] {
+        if (!e || !info) b2::fail(B2_ERR_INVALID, "null argument");
+        b2::engine_info(e->impl, info);
+    });
+}
+
+int b2_engine_spmv(b2_engine* e, int32_t which, const double* x, double* y) {
+    return b2::guarded([&] {
+        if (!e || !x || !y || (which != 0 && which != 1)) b2::fail(B2_ERR_INVALID, "bad argument");
+        b2::engine_spmv(e->impl, which, x, y);
+    });
+}
+
+int b2_engine_spmv_bench(b2_engine* e, int32_t which, int32_t precision, int32_t reps, void* stream,
+                         double* avg_ms) {
+    return b2::guarded([&] {
+        if (!e || !avg_ms || (which != 0 && which != 1) || reps < 0) b2::fail(B2_ERR_INVALID, "bad argument");
+        b2::engine_spmv_bench(e->impl, which, precision, reps, stream, avg_ms);
+    });
+}
+
+int b2_scale(const b2_lp_view* lp, int32_t ruiz_passes, double* val_s, double* c_s, double* rL_s, double* rU_s,
+             double* l_s, double* u_s, double* Dr, double* Dc) {
+    return b2::guarded([&] {
+        if (!lp) b2::fail(B2_ERR_INVALID, "null argument");
+        b2::scale_lp(*lp, ruiz_passes, val_s, c_s, rL_s, rU_s, l_s, u_s, Dr, Dc);
+    });
+}
+
+int b2_gen_random_lp(int32_t m, int32_t n, int32_t k, uint64_t seed, int32_t fp32_values, int32_t* row,
+                     int32_t* col, double* val, double* c, double* rL, double* rU, double* l, double* u) {
+    return b2::guarded([&] { b2::gen_random_lp(m, n, k, seed, fp32_values != 0, row, col, val, c, rL, rU, l, u); });
+}
+
+int b2_gen_transport(int32_t S, int32_t D, uint64_t seed, int32_t* row, int32_t* col, double* val, double* c,
+                     double* rL, double* rU, double* l, double* u) {
+    return b2::guarded([&] { b2::gen_transport(S, D, seed, row, col, val, c, rL, rU, l, u); });
+}
+
+}  // extern "C"

@@ -1,0 +1,388 @@
+// host_prep.cpp -- host side of the engine that needs no GPU:
+//   * validation of the PDLP form handed over by solve_pdhg_gpu's callers,
+//   * the device layout (row/column permutations and the sliced-ELL format of
+//     A and A^T, with per-row/per-column vectors in the same permuted order),
+//   * Ruiz + Pock-Chambolle scaling (same algorithm as src/scaling.cpp:25-84),
+//   * seeded generators for the benchmark LP shapes.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <limits>
+#include <numeric>
+#include <string>
+#include <vector>
+
+#include "internal.h"
+
+namespace b2 {
+
+namespace {
+
+constexpr double kInf = std::numeric_limits<double>::infinity();
+
+// CSR with the stable fill order of include/sparse.hpp:24-40 (entries of a row
+// keep their COO order).
+void coo_to_csr(int64_t rows, int64_t nnz, const int32_t* r, const int32_t* c, const double* v,
+                std::vector<int64_t>& ptr, std::vector<int32_t>& idx, std::vector<double>& val) {
+    ptr.assign(rows + 1, 0);
+    for (int64_t k = 0; k < nnz; ++k) ptr[r[k] + 1]++;
+    for (int64_t i = 0; i < rows; ++i) ptr[i + 1] += ptr[i];
+    idx.resize(nnz);
+    val.resize(nnz);
+    std::vector<int64_t> cur(ptr.begin(), ptr.end() - 1);
+    for (int64_t k = 0; k < nnz; ++k) {
+        int64_t p = cur[r[k]]++;
+        idx[p] = c[k];
+        val[p] = v[k];
+    }
+}
+
+// Rows sorted by length, longest first, inside windows of `window` rows; the
+// window keeps neighbouring rows together so gathers keep their locality.
+std::vector<int32_t> sigma_sort(const std::vector<int64_t>& ptr, int window) {
+    const int32_t rows = (int32_t)ptr.size() - 1;
+    std::vector<int32_t> perm(rows);
+    std::iota(perm.begin(), perm.end(), 0);
+    if (window <= 1) return perm;
+    for (int32_t w0 = 0; w0 < rows; w0 += window) {
+        int32_t w1 = std::min<int64_t>((int64_t)w0 + window, rows);
+        std::stable_sort(perm.begin() + w0, perm.begin() + w1, [&](int32_t a, int32_t b) {
+            return ptr[a + 1] - ptr[a] > ptr[b + 1] - ptr[b];
+        });
+    }
+    return perm;
+}
+
+int pick_lanes(int64_t len, int lane_target) {
+    int g = 1;
+    while (g < 32 && (len + g - 1) / g > lane_target) g <<= 1;
+    return g;
+}
+
+// Builds the sliced format of the rows `perm` (device order) of a CSR whose
+// column indices are mapped through `inv_col`.
+void build_sell(const std::vector<int64_t>& ptr, const std::vector<int32_t>& idx, const std::vector<double>& val,
+                const std::vector<int32_t>& perm, const std::vector<int32_t>& inv_col, int n_cols, int lane_target,
+                bool keep64, SellHost& S) {
+    const int32_t rows = (int32_t)perm.size();
+    S.n_rows = rows;
+    S.n_cols = n_cols;
+    S.slice.clear();
+    // pass 1: slice shapes
+    struct Shape { int32_t row0, nrows, lg; int64_t len, blk; };
+    std::vector<Shape> shapes;
+    int64_t blk = 0;
+    for (int32_t i = 0; i < rows;) {
+        const int32_t r0 = perm[i];
+        const int g = pick_lanes(ptr[r0 + 1] - ptr[r0], lane_target);
+        const int32_t nr = std::min<int32_t>(32 / g, rows - i);
+        int64_t lmax = 0;
+        for (int32_t t = 0; t < nr; ++t) lmax = std::max<int64_t>(lmax, ptr[perm[i + t] + 1] - ptr[perm[i + t]]);
+        const int64_t len = (lmax + g - 1) / g;
+        if (len > (int64_t)kLenMask) fail(B2_ERR_UNSUPPORTED, "row too long for the sliced format");
+        int lg = 0;
+        while ((1 << lg) < g) ++lg;
+        shapes.push_back({i, nr, lg, len, blk});
+        blk += len;
+        i += nr;
+    }
+    if (blk >= (int64_t)std::numeric_limits<uint32_t>::max()) fail(B2_ERR_UNSUPPORTED, "matrix too large");
+    S.padded = blk * 32;
+    S.col.assign((size_t)S.padded, 0u);
+    S.val32.assign((size_t)S.padded, 0.0f);
+    if (keep64) S.val64.assign((size_t)S.padded, 0.0);
+    else S.val64.clear();
+    S.slice.resize(shapes.size() * 4);
+    // pass 2: fill
+    for (size_t s = 0; s < shapes.size(); ++s) {
+        const Shape& sh = shapes[s];
+        const int g = 1 << sh.lg;
+        S.slice[4 * s + 0] = sh.row0;
+        S.slice[4 * s + 1] = (int32_t)((uint32_t)sh.len | ((uint32_t)sh.lg << kLenBits));
+        S.slice[4 * s + 2] = (int32_t)(uint32_t)sh.blk;
+        S.slice[4 * s + 3] = 0;
+        for (int lane = 0; lane < 32; ++lane) {
+            const int32_t rl = lane / g, sub = lane % g;
+            uint32_t last_col = 0;
+            int64_t k = 0;
+            if (rl < sh.nrows) {
+                const int32_t r = perm[sh.row0 + rl];
+                const int64_t b = ptr[r], e = ptr[r + 1];
+                if (e > b) last_col = (uint32_t)inv_col[idx[b]];
+                for (int64_t p = b + sub; p < e; p += g, ++k) {
+                    const size_t pos = (size_t)((sh.blk + k) * 32 + lane);
+                    last_col = (uint32_t)inv_col[idx[p]];
+                    S.col[pos] = last_col;
+                    S.val32[pos] = (float)val[p];
+                    if (keep64) S.val64[pos] = val[p];
+                }
+            }
+            for (; k < sh.len; ++k) S.col[(size_t)((sh.blk + k) * 32 + lane)] = last_col;  // value stays 0
+        }
+    }
+}
+
+double finite_inf_norm(const double* v, int64_t len) {
+    double m = 0.0;
+    for (int64_t i = 0; i < len; ++i)
+        if (std::isfinite(v[i])) m = std::max(m, std::fabs(v[i]));
+    return m;
+}
+
+}  // namespace
+
+void build_layout(const b2_lp_view& U, const b2_lp_view& S, const double* Dr, const double* Dc,
+                  const BuildParams& bp, Layout& L) {
+    const int32_t m = U.m, n = U.n;
+    const int64_t nnz = U.nnz;
+    if (m < 0 || n < 0 || nnz < 0) fail(B2_ERR_INVALID, "negative dimension");
+    if (S.m != m || S.n != n || S.nnz != nnz) fail(B2_ERR_INVALID, "scaled form does not match the unscaled form");
+    if (nnz > 0 && (!U.row_idx || !U.col_idx || !U.val || !S.val)) fail(B2_ERR_INVALID, "null matrix pointer");
+    if ((n > 0 && (!U.c || !U.l || !U.u || !S.c || !S.l || !S.u || !Dc)) ||
+        (m > 0 && (!U.rL || !U.rU || !S.rL || !Dr)))
+        fail(B2_ERR_INVALID, "null vector pointer");
+    for (int64_t k = 0; k < nnz; ++k) {
+        if (U.row_idx[k] < 0 || U.row_idx[k] >= m || U.col_idx[k] < 0 || U.col_idx[k] >= n)
+            fail(B2_ERR_INVALID, "matrix index out of range at entry " + std::to_string(k));
+        if (!std::isfinite(U.val[k]) || !std::isfinite(S.val[k]))
+            fail(B2_ERR_NONFINITE, "non-finite matrix value at entry " + std::to_string(k));
+    }
+    // PDLP-form invariant (src/pdlp.cpp:59-62): rL finite, rU == rL or +inf.
+    for (int32_t i = 0; i < m; ++i) {
+        if (!std::isfinite(U.rL[i])) fail(B2_ERR_NONFINITE, "rL must be finite in the PDLP form (row " + std::to_string(i) + ")");
+        if (!(U.rU[i] == U.rL[i] || (std::isinf(U.rU[i]) && U.rU[i] > 0)))
+            fail(B2_ERR_INVALID, "row " + std::to_string(i) + " is neither an equality nor a >= row");
+        if (!(Dr[i] > 0) || !std::isfinite(Dr[i])) fail(B2_ERR_INVALID, "Dr must be positive and finite");
+    }
+    for (int32_t j = 0; j < n; ++j) {
+        if (!std::isfinite(U.c[j]) || !std::isfinite(S.c[j])) fail(B2_ERR_NONFINITE, "non-finite cost at column " + std::to_string(j));
+        if (std::isnan(U.l[j]) || std::isnan(U.u[j]) || U.l[j] > U.u[j])
+            fail(B2_ERR_INVALID, "bad bounds at column " + std::to_string(j));
+        if (!(Dc[j] > 0) || !std::isfinite(Dc[j])) fail(B2_ERR_INVALID, "Dc must be positive and finite");
+        const double want = Dc[j] * U.c[j];
+        if (std::fabs(S.c[j] - want) > 1e-9 * (1.0 + std::fabs(want)))
+            fail(B2_ERR_INVALID, "scaled cost is not Dc * cost at column " + std::to_string(j));
+    }
+
+    L.m = m; L.n = n; L.nnz = nnz;
+    std::vector<int64_t> aptr, tptr;
+    std::vector<int32_t> aidx, tidx;
+    std::vector<double> aval, tval;
+    coo_to_csr(m, nnz, U.row_idx, U.col_idx, U.val, aptr, aidx, aval);
+    coo_to_csr(n, nnz, U.col_idx, U.row_idx, U.val, tptr, tidx, tval);
+
+    L.exact32 = true;
+    for (int64_t k = 0; k < nnz; ++k)
+        if ((double)(float)U.val[k] != U.val[k]) { L.exact32 = false; break; }
+
+    const int window = bp.sigma_window > 0 ? bp.sigma_window : 1024;
+    const int target = bp.lane_target > 0 ? bp.lane_target : 16;
+    L.perm_r = sigma_sort(aptr, window);
+    L.perm_c = sigma_sort(tptr, window);
+    L.inv_r.assign(m, 0);
+    L.inv_c.assign(n, 0);
+    for (int32_t i = 0; i < m; ++i) L.inv_r[L.perm_r[i]] = i;
+    for (int32_t j = 0; j < n; ++j) L.inv_c[L.perm_c[j]] = j;
+
+    build_sell(aptr, aidx, aval, L.perm_r, L.inv_c, n, target, !L.exact32, L.A);
+    build_sell(tptr, tidx, tval, L.perm_c, L.inv_r, m, target, !L.exact32, L.AT);
+
+    L.b.resize(m); L.rU.resize(m); L.dr2.resize(m);
+    for (int32_t i = 0; i < m; ++i) {
+        const int32_t o = L.perm_r[i];
+        L.b[i] = U.rL[o];
+        L.rU[i] = U.rU[o];
+        const double w = Dr[o] * Dr[o];
+        L.dr2[i] = (U.rL[o] != U.rU[o]) ? -w : w;
+    }
+    L.c.resize(n); L.l.resize(n); L.u.resize(n); L.dc2.resize(n); L.x0.resize(n);
+    for (int32_t j = 0; j < n; ++j) {
+        const int32_t o = L.perm_c[j];
+        L.c[j] = U.c[o];
+        L.l[j] = U.l[o];
+        L.u[j] = U.u[o];
+        L.dc2[j] = Dc[o] * Dc[o];
+        // initial point of include/pdlp_algo.hpp:69, mapped to unscaled space
+        L.x0[j] = Dc[o] * std::min(std::max(0.0, S.l[o]), S.u[o]);
+    }
+    // step size and primal weight seeds (include/pdlp_algo.hpp:70-77), on the scaled form
+    double amax = 0.0;
+    for (int64_t k = 0; k < nnz; ++k) amax = std::max(amax, std::fabs(S.val[k]));
+    L.eta0 = amax > 0 ? 1.0 / amax : 1.0;
+    double cn = 0.0, bn = 0.0;
+    for (int32_t j = 0; j < n; ++j) cn += S.c[j] * S.c[j];
+    for (int32_t i = 0; i < m; ++i)
+        if (std::isfinite(S.rL[i])) bn += S.rL[i] * S.rL[i];
+    cn = std::sqrt(cn);
+    bn = std::sqrt(bn);
+    L.omega0 = (cn > 1e-10 && bn > 1e-10) ? cn / bn : 1.0;
+    // KKT denominators of src/verify.cpp:39,56 (unscaled form)
+    L.denom_p = 1.0 + std::max(finite_inf_norm(U.rL, m), finite_inf_norm(U.rU, m));
+    L.denom_d = 1.0 + finite_inf_norm(U.c, n);
+    L.obj_offset = U.obj_offset;
+}
+
+// ----------------------------------------------------------------- scaling
+void scale_lp(const b2_lp_view& lp, int ruiz_passes, double* val_s, double* c_s, double* rL_s, double* rU_s,
+              double* l_s, double* u_s, double* Dr, double* Dc) {
+    const int32_t m = lp.m, n = lp.n;
+    const int64_t nnz = lp.nnz;
+    for (int64_t k = 0; k < nnz; ++k)
+        if (lp.row_idx[k] < 0 || lp.row_idx[k] >= m || lp.col_idx[k] < 0 || lp.col_idx[k] >= n)
+            fail(B2_ERR_INVALID, "matrix index out of range");
+    const int32_t* R = lp.row_idx;
+    const int32_t* Cc = lp.col_idx;
+    std::copy(lp.val, lp.val + nnz, val_s);
+    std::fill(Dr, Dr + m, 1.0);
+    std::fill(Dc, Dc + n, 1.0);
+    std::vector<double> rs(m), cs(n);
+    for (int pass = 0; pass < ruiz_passes; ++pass) {
+        std::fill(rs.begin(), rs.end(), 0.0);
+        for (int64_t k = 0; k < nnz; ++k) rs[R[k]] = std::max(rs[R[k]], std::fabs(val_s[k]));
+        for (int32_t i = 0; i < m; ++i) rs[i] = rs[i] > 0 ? 1.0 / std::sqrt(rs[i]) : 1.0;
+        for (int64_t k = 0; k < nnz; ++k) val_s[k] = val_s[k] * rs[R[k]];
+        for (int32_t i = 0; i < m; ++i) Dr[i] *= rs[i];
+        std::fill(cs.begin(), cs.end(), 0.0);
+        for (int64_t k = 0; k < nnz; ++k) cs[Cc[k]] = std::max(cs[Cc[k]], std::fabs(val_s[k]));
+        for (int32_t j = 0; j < n; ++j) cs[j] = cs[j] > 0 ? 1.0 / std::sqrt(cs[j]) : 1.0;
+        for (int64_t k = 0; k < nnz; ++k) val_s[k] = val_s[k] * cs[Cc[k]];
+        for (int32_t j = 0; j < n; ++j) Dc[j] *= cs[j];
+    }
+    std::fill(rs.begin(), rs.end(), 0.0);
+    std::fill(cs.begin(), cs.end(), 0.0);
+    for (int64_t k = 0; k < nnz; ++k) rs[R[k]] += std::fabs(val_s[k]);
+    for (int64_t k = 0; k < nnz; ++k) cs[Cc[k]] += std::fabs(val_s[k]);
+    for (int32_t i = 0; i < m; ++i) rs[i] = std::sqrt(rs[i] > 0 ? 1.0 / rs[i] : 1.0);
+    for (int32_t j = 0; j < n; ++j) cs[j] = std::sqrt(cs[j] > 0 ? 1.0 / cs[j] : 1.0);
+    for (int64_t k = 0; k < nnz; ++k) val_s[k] = val_s[k] * rs[R[k]] * cs[Cc[k]];
+    for (int32_t i = 0; i < m; ++i) Dr[i] *= rs[i];
+    for (int32_t j = 0; j < n; ++j) Dc[j] *= cs[j];
+    for (int32_t j = 0; j < n; ++j) {
+        c_s[j] = Dc[j] * lp.c[j];
+        l_s[j] = lp.l[j] / Dc[j];
+        u_s[j] = lp.u[j] / Dc[j];
+    }
+    for (int32_t i = 0; i < m; ++i) {
+        rL_s[i] = Dr[i] * lp.rL[i];
+        rU_s[i] = Dr[i] * lp.rU[i];
+    }
+}
+
+// -------------------------------------------------------------- generators
+namespace {
+
+// xoshiro256** seeded through splitmix64 (Blackman & Vigna's published
+// generators), so every benchmark input is reproducible from its seed.
+struct Rng {
+    uint64_t s[4];
+    explicit Rng(uint64_t seed) {
+        uint64_t z = seed;
+        for (auto& w : s) {
+            z += 0x9E3779B97F4A7C15ull;
+            uint64_t t = z;
+            t = (t ^ (t >> 30)) * 0xBF58476D1CE4E5B9ull;
+            t = (t ^ (t >> 27)) * 0x94D049BB133111EBull;
+            w = t ^ (t >> 31);
+        }
+    }
+    static uint64_t rotl(uint64_t x, int k) { return (x << k) | (x >> (64 - k)); }
+    uint64_t next() {
+        const uint64_t r = rotl(s[1] * 5, 7) * 9;
+        const uint64_t t = s[1] << 17;
+        s[2] ^= s[0]; s[3] ^= s[1]; s[1] ^= s[2]; s[0] ^= s[3];
+        s[2] ^= t;
+        s[3] = rotl(s[3], 45);
+        return r;
+    }
+    double uniform() { return (double)(next() >> 11) * 0x1.0p-53; }           // [0, 1)
+    int64_t below(int64_t n) { return (int64_t)(uniform() * (double)n); }      // [0, n)
+    double normal() {                                                         // Marsaglia polar
+        for (;;) {
+            double a = 2.0 * uniform() - 1.0, b = 2.0 * uniform() - 1.0, q = a * a + b * b;
+            if (q > 0.0 && q < 1.0) return a * std::sqrt(-2.0 * std::log(q) / q);
+        }
+    }
+};
+
+}  // namespace
+
+void gen_random_lp(int m, int n, int k, uint64_t seed, bool fp32_values, int32_t* row, int32_t* col, double* val,
+                   double* c, double* rL, double* rU, double* l, double* u) {
+    if (m <= 0 || n <= 0 || k <= 0 || k > m) fail(B2_ERR_INVALID, "bad generator sizes");
+    Rng rng(seed);
+    std::vector<int32_t> pick(k);
+    for (int32_t j = 0; j < n; ++j) {
+        for (int t = 0; t < k; ++t) {
+            int32_t r;
+            bool dup;
+            do {
+                r = (int32_t)rng.below(m);
+                dup = false;
+                for (int q = 0; q < t; ++q) dup |= pick[q] == r;
+            } while (dup);
+            pick[t] = r;
+            double v;
+            do {
+                v = 2.0 * rng.uniform() - 1.0;
+                if (fp32_values) v = (double)(float)v;
+            } while (v == 0.0);
+            const int64_t p = (int64_t)j * k + t;
+            row[p] = r;
+            col[p] = j;
+            val[p] = v;
+        }
+    }
+    std::vector<double> x0(n), y0(m);
+    for (int32_t j = 0; j < n; ++j) x0[j] = 5.0 * rng.uniform();
+    for (int32_t i = 0; i < m; ++i) y0[i] = rng.normal();
+    std::fill(rL, rL + m, 0.0);
+    for (int64_t p = 0; p < (int64_t)n * k; ++p) rL[row[p]] += val[p] * x0[col[p]];
+    for (int32_t j = 0; j < n; ++j) {
+        double s = 0.0;
+        for (int t = 0; t < k; ++t) {
+            const int64_t p = (int64_t)j * k + t;
+            s += val[p] * y0[row[p]];
+        }
+        c[j] = s + rng.uniform();
+        l[j] = 0.0;
+        u[j] = 10.0;
+    }
+    std::copy(rL, rL + m, rU);
+}
+
+void gen_transport(int S, int D, uint64_t seed, int32_t* row, int32_t* col, double* val, double* c, double* rL,
+                   double* rU, double* l, double* u) {
+    if (S < 1 || D < 1) fail(B2_ERR_INVALID, "bad transport sizes");
+    Rng rng(seed);
+    std::vector<int64_t> supply(S), demand(D);
+    int64_t total = 0;
+    for (int i = 0; i < S; ++i) { supply[i] = 100 + rng.below(901); total += supply[i]; }
+    std::vector<double> w(D);
+    double wsum = 0.0;
+    for (int j = 0; j < D; ++j) { w[j] = 0.5 + rng.uniform(); wsum += w[j]; }
+    int64_t assigned = 0;
+    for (int j = 0; j < D; ++j) {
+        demand[j] = std::max<int64_t>(1, (int64_t)std::floor((double)total * w[j] / wsum));
+        assigned += demand[j];
+    }
+    // integer partition: hand the remainder out one unit at a time, round robin
+    for (int64_t r = total - assigned, j = 0; r != 0; j = (j + 1) % D) {
+        if (r > 0) { demand[j]++; r--; }
+        else if (demand[j] > 1) { demand[j]--; r++; }
+    }
+    const int64_t n = (int64_t)S * D;
+    for (int i = 0; i < S; ++i)
+        for (int j = 0; j < D; ++j) {
+            const int64_t a = (int64_t)i * D + j;
+            row[2 * a] = i;         col[2 * a] = (int32_t)a;     val[2 * a] = 1.0;
+            row[2 * a + 1] = S + j; col[2 * a + 1] = (int32_t)a; val[2 * a + 1] = 1.0;
+            c[a] = (double)(1 + rng.below(100));
+            l[a] = 0.0;
+            u[a] = kInf;
+        }
+    (void)n;
+    for (int i = 0; i < S; ++i) rL[i] = rU[i] = (double)supply[i];
+    for (int j = 0; j < D; ++j) rL[S + j] = rU[S + j] = (double)demand[j];
+}
+
+}  // namespace b2

@@ -1,0 +1,88 @@
+// internal.h -- shared declarations of the host preparation (host_prep.cpp)
+// and the CUDA engine (engine.cu). Not part of the C ABI.
+#pragma once
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "b200_pdlp.h"
+
+namespace b2 {
+
+// Error carried to the C ABI as (code, message).
+struct Error {
+    int code;
+    std::string msg;
+};
+[[noreturn]] void fail(int code, const std::string& msg);
+void set_last_error(const std::string& msg);
+
+// Sliced ELL with a per-slice lane count ("lanes per row", g = 1..32).
+//
+// A slice is one warp's unit of work: 32/g consecutive rows (in the permuted
+// order), each row spread round-robin over g lanes. Entry e of a row lives in
+// lane (row_in_slice * g + e % g) at step e / g; step k of lane l is stored at
+// element 32 * (blk + k) + l, i.e. column-major inside the slice, so a warp's
+// 32 lanes read 32 consecutive words per step. len = steps of the slice.
+// slice[s] = {row0, len | (log2 g) << 27, blk, 0}.
+struct SellHost {
+    int32_t n_rows = 0, n_cols = 0;
+    std::vector<int32_t> slice;       // 4 ints per slice
+    std::vector<uint32_t> col;        // padded, 32 * total blocks
+    std::vector<float> val32;
+    std::vector<double> val64;        // only when values are not exact in FP32
+    int64_t padded = 0;               // stored entries including padding
+    int64_t n_slices() const { return (int64_t)slice.size() / 4; }
+};
+
+constexpr int kLenBits = 27;
+constexpr uint32_t kLenMask = (1u << kLenBits) - 1;
+
+// Everything the device needs, in device (permuted) order.
+struct Layout {
+    int32_t m = 0, n = 0;
+    int64_t nnz = 0;
+    std::vector<int32_t> perm_r;      // device row i  -> caller row perm_r[i]
+    std::vector<int32_t> perm_c;      // device col j  -> caller col perm_c[j]
+    std::vector<int32_t> inv_r, inv_c;
+    SellHost A, AT;
+    bool exact32 = true;
+    // rows
+    std::vector<double> b, rU;        // b = rL of the PDLP form
+    std::vector<double> dr2;          // Dr^2, negated on inequality rows
+    // cols
+    std::vector<double> c, l, u, x0;  // x0 = Dc * clamp(0, l_s, u_s)
+    std::vector<double> dc2;          // Dc^2
+    // scalars
+    double eta0 = 1.0, omega0 = 1.0, denom_p = 1.0, denom_d = 1.0, obj_offset = 0.0;
+};
+
+struct BuildParams {
+    int lane_target = 16;   // entries per lane that decides lanes-per-row
+    int sigma_window = 1024;
+};
+
+// Validates the PDLP form and builds the device layout. Throws Error.
+void build_layout(const b2_lp_view& U, const b2_lp_view& S, const double* Dr, const double* Dc,
+                  const BuildParams& bp, Layout& L);
+
+void scale_lp(const b2_lp_view& lp, int ruiz_passes, double* val_s, double* c_s, double* rL_s, double* rU_s,
+              double* l_s, double* u_s, double* Dr, double* Dc);
+
+void gen_random_lp(int m, int n, int k, uint64_t seed, bool fp32_values, int32_t* row, int32_t* col, double* val,
+                   double* c, double* rL, double* rU, double* l, double* u);
+void gen_transport(int S, int D, uint64_t seed, int32_t* row, int32_t* col, double* val, double* c, double* rL,
+                   double* rU, double* l, double* u);
+
+// The CUDA engine (engine.cu). All functions throw Error.
+struct EngineImpl;
+EngineImpl* engine_create(const b2_lp_view& U, const b2_lp_view& S, const double* Dr, const double* Dc,
+                          const b2_solve_opts& o);
+void engine_destroy(EngineImpl* e);
+void engine_solve(EngineImpl* e, const b2_solve_opts& o, const volatile int32_t* stop, double* x, double* y,
+                  b2_result* r);
+void engine_info(EngineImpl* e, b2_engine_info* info);
+void engine_spmv(EngineImpl* e, int which, const double* x, double* y);
+void engine_spmv_bench(EngineImpl* e, int which, int precision, int reps, void* stream, double* avg_ms);
+
+}  // namespace b2

@@ -1,0 +1,99 @@
+"""The C-ABI library without a GPU: it loads, exports what include/b200_pdlp.h
+declares, and rejects malformed input with the documented status codes."""
+import ctypes as C
+import os
+import re
+
+import numpy as np
+import pytest
+
+import b200pdlp as B
+from conftest import ROOT, gpu_available, load_fixture
+
+
+def declared_functions():
+    src = open(os.path.join(ROOT, "include", "b200_pdlp.h")).read()
+    src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+    return sorted(set(re.findall(r"\b(b2_[a-z0-9_]+)\s*\(", src)))
+
+
+def test_library_loads_and_exports_every_declared_symbol():
+    lib = B.lib()
+    names = declared_functions()
+    assert len(names) >= 12
+    missing = [n for n in names if not hasattr(lib, n)]
+    assert not missing, missing
+    assert set(names) == set(B.EXPORTED)
+
+
+def test_version_and_defaults():
+    assert "sm_100a" in B.version()
+    o = B.default_opts()
+    assert (o.max_iterations, o.check_every, o.tol) == (200000, 64, 1e-6)
+    assert o.precision == B.PREC_MIXED
+
+
+def _view_args(U, S):
+    return B.RangedLP.like(U), B.RangedLP.like(S)
+
+
+def test_rejects_out_of_range_index():
+    U, S, Dr, Dc = load_fixture("afiro")
+    U2 = B.RangedLP.like(U)
+    U2.col = U2.col.copy()
+    U2.col[0] = U.n + 5
+    with pytest.raises(B.B2Error) as e:
+        B.solve_pdhg_gpu(U2, S, Dr, Dc)
+    assert e.value.code == B.B2_ERR_INVALID
+
+
+def test_rejects_nonfinite_value():
+    U, S, Dr, Dc = load_fixture("afiro")
+    U2 = B.RangedLP.like(U)
+    U2.val = U2.val.copy()
+    U2.val[1] = np.nan
+    with pytest.raises(B.B2Error) as e:
+        B.solve_pdhg_gpu(U2, S, Dr, Dc)
+    assert e.value.code == B.B2_ERR_NONFINITE
+    U3 = B.RangedLP.like(U)
+    U3.c = U3.c.copy()
+    U3.c[0] = np.inf
+    with pytest.raises(B.B2Error) as e:
+        B.solve_pdhg_gpu(U3, S, Dr, Dc)
+    assert e.value.code == B.B2_ERR_NONFINITE
+
+
+def test_rejects_non_pdlp_form():
+    """A <= row (rL = -inf) is not a PDLP-form row (src/pdlp.cpp:59-62)."""
+    U, S, Dr, Dc = load_fixture("afiro")
+    U2 = B.RangedLP.like(U)
+    U2.rL = U2.rL.copy()
+    U2.rL[0] = -np.inf
+    with pytest.raises(B.B2Error) as e:
+        B.solve_pdhg_gpu(U2, S, Dr, Dc)
+    assert e.value.code == B.B2_ERR_NONFINITE
+
+
+def test_rejects_inconsistent_scaling():
+    U, S, Dr, Dc = load_fixture("afiro")
+    S2 = B.RangedLP.like(S)
+    S2.c = S2.c * 2.0 + 1.0
+    with pytest.raises(B.B2Error) as e:
+        B.solve_pdhg_gpu(U, S2, Dr, Dc)
+    assert e.value.code == B.B2_ERR_INVALID
+
+
+@pytest.mark.skipif(gpu_available(), reason="this box has a GPU")
+def test_no_device_is_reported_not_hidden():
+    """No CPU fallback: without a device the solve fails loudly."""
+    U, S, Dr, Dc = load_fixture("afiro")
+    with pytest.raises(B.B2Error) as e:
+        B.solve_pdhg_gpu(U, S, Dr, Dc)
+    assert e.value.code in (B.B2_ERR_NO_DEVICE, B.B2_ERR_CUDA)
+
+
+def test_stop_flag_word_layout():
+    f = B.StopFlag()
+    assert not f.is_set()
+    f.set()
+    assert C.c_int32.from_address(f.ptr).value == 1

@@ -1,0 +1,104 @@
+"""Host-side preparation of the product (no GPU): scaling, PDLP form and the
+benchmark generators, checked against the oracle and the reference."""
+import numpy as np
+import pytest
+
+import b200pdlp as B
+import oracle as O
+from conftest import as_form, fixture_names, load_fixture
+
+
+@pytest.mark.parametrize("name", fixture_names())
+def test_product_scaling_bitexact_with_oracle(name):
+    """b2_scale restates src/scaling.cpp:25-84; it must give the same bits."""
+    U, S, Dr, Dc = load_fixture(name)
+    s, dr, dc = B.scale(B.RangedLP.like(U))
+    np.testing.assert_array_equal(s.val, S.val)
+    np.testing.assert_array_equal(s.c, S.c)
+    np.testing.assert_array_equal(s.l, S.l)
+    np.testing.assert_array_equal(s.u, S.u)
+    np.testing.assert_array_equal(s.rL, S.rL)
+    np.testing.assert_array_equal(dr, Dr)
+    np.testing.assert_array_equal(dc, Dc)
+
+
+def test_product_scaling_random_family():
+    lp = B.gen_random_lp(200, 600, 5, 11, False)
+    s, dr, dc = B.scale(lp)
+    s2, dr2, dc2 = O.scale(as_form(lp))
+    np.testing.assert_array_equal(s.val, s2.val)
+    np.testing.assert_array_equal(dr, dr2)
+    np.testing.assert_array_equal(dc, dc2)
+
+
+def _mixed_rows_lp():
+    # rows: E, L, G, ranged, free, E ; columns with finite / infinite bounds
+    rng = np.random.default_rng(5)
+    m, n = 6, 5
+    row, col, val = [], [], []
+    for i in range(m):
+        for j in rng.choice(n, 3, replace=False):
+            row.append(i); col.append(int(j)); val.append(float(rng.uniform(-2, 2)))
+    inf = np.inf
+    rL = np.array([1.0, -inf, 0.5, -1.0, -inf, 2.0])
+    rU = np.array([1.0, 3.0, inf, 4.0, inf, 2.0])
+    l = np.array([0.0, -inf, -1.0, 0.0, -inf])
+    u = np.array([5.0, inf, 2.0, inf, 3.0])
+    c = rng.normal(size=n)
+    return B.RangedLP(m, n, np.array(row), np.array(col), np.array(val), c, rL, rU, l, u, 1.5)
+
+
+@pytest.mark.skipif(not O.reference_available(), reason="reference library not built here")
+def test_build_pdlp_form_matches_reference():
+    """Row order, signs, slack columns and dropped free rows as src/pdlp.cpp:8-82."""
+    lp = _mixed_rows_lp()
+    form, meta = B.build_pdlp_form(lp)
+    P = O.RefProblem.from_form(as_form(lp), use_presolve=False)
+    ref = P.form(P.PDLP_FORM)
+    assert (form.m, form.n, form.nnz) == (ref.m, ref.n, ref.nnz)
+    key = lambda f: sorted(zip(f.row.tolist(), f.col.tolist(), f.val.tolist()))  # noqa: E731
+    assert key(form) == key(ref)
+    for a in ("c", "rL", "rU", "l", "u"):
+        np.testing.assert_array_equal(getattr(form, a), getattr(ref, a))
+    assert form.obj_offset == ref.obj_offset
+
+
+def test_transport_generator_shape_and_balance():
+    S, D = 20, 7
+    lp = B.gen_transport(S, D, 3)
+    assert (lp.m, lp.n, lp.nnz) == (S + D, S * D, 2 * S * D)
+    assert np.all(lp.val == 1.0)
+    supply, demand = lp.rL[:S], lp.rL[S:]
+    assert np.all((supply >= 100) & (supply <= 1000)) and np.all(supply == np.round(supply))
+    assert supply.sum() == demand.sum()
+    assert np.all(demand >= 1) and np.all(demand == np.round(demand))
+    assert np.all((lp.c >= 1) & (lp.c <= 100)) and np.all(lp.c == np.round(lp.c))
+    assert np.all(lp.l == 0) and np.all(np.isinf(lp.u))
+    counts = np.bincount(lp.col, minlength=lp.n)
+    assert np.all(counts == 2)
+
+
+def test_random_generator_shape_and_determinism():
+    m, n, k = 50, 150, 6
+    a = B.gen_random_lp(m, n, k, 9, True)
+    b = B.gen_random_lp(m, n, k, 9, True)
+    for f in ("row", "col", "val", "c", "rL"):
+        np.testing.assert_array_equal(getattr(a, f), getattr(b, f))
+    assert np.all(np.bincount(a.col, minlength=n) == k)
+    for j in range(n):  # distinct rows per column
+        rows = a.row[a.col == j]
+        assert len(set(rows.tolist())) == k
+    assert np.all(np.abs(a.val) <= 1.0) and np.all(a.val != 0)
+    assert np.all(a.val == a.val.astype(np.float32).astype(np.float64))
+    np.testing.assert_array_equal(a.rL, a.rU)
+    assert np.all(a.l == 0) and np.all(a.u == 10)
+
+
+def test_random_lp_is_feasible_by_construction():
+    """b = A x0 for some x0 in [0,5]^n: the LP is feasible (the CPU oracle solves it)."""
+    lp = B.gen_random_lp(40, 120, 4, 21, False)
+    U, S, Dr, Dc, _ = B.prepare(lp)
+    r = O.pdlp_run(as_form(U), as_form(S), Dr, Dc, tol=1e-7, max_iterations=200000)
+    assert r["converged"]
+    v = O.verify(as_form(U), r["x"], r["y"])
+    assert max(v["eps_P"], v["eps_D"], v["eps_G"]) <= 1e-7

@@ -1,0 +1,84 @@
+"""Pins the oracle: the C restatement (oracle/pdlp_oracle.c) against the golden
+fixtures made by the reference itself, and -- where the reference library is
+built (oracle/_ref) -- against the reference directly, bit for bit."""
+import numpy as np
+import pytest
+
+import oracle as O
+from conftest import fixture_names, golden_index, load_fixture, random_case
+
+FIX = fixture_names()
+
+
+@pytest.mark.parametrize("name", FIX)
+def test_restatement_reproduces_reference_pdlp(name):
+    """Same iterations, restarts, residuals and objective as the reference's
+    solve_pdhg on the reference's own fixture (tests/run_checks.cpp cases)."""
+    g = golden_index()["fixtures"][name]["pdlp"]["1e-06"]
+    U, S, Dr, Dc = load_fixture(name)
+    r = O.pdlp_run(U, S, Dr, Dc, max_iterations=500000, check_every=64, tol=1e-6)
+    assert r["iterations"] == g["iterations"]
+    assert r["restarts"] == g["restarts"]
+    assert r["converged"] == g["converged"]
+    assert r["eps_P"] == pytest.approx(g["eps_P"], rel=1e-9, abs=1e-300)
+    v = O.verify(U, r["x"], r["y"])
+    assert v["objective"] == pytest.approx(g["form_objective"], rel=1e-12)
+
+
+@pytest.mark.skipif(not O.reference_available(), reason="reference library not built here")
+@pytest.mark.parametrize("name", ["afiro", "sc50a", "blend", "beaconfd", "israel"])
+def test_restatement_bitexact_with_reference(name):
+    U, S, Dr, Dc = load_fixture(name)
+    r = O.pdlp_run(U, S, Dr, Dc, max_iterations=500000, tol=1e-6)
+    lib = O.reference()
+    h = lib.ref_from_arrays(U.m, U.n, U.nnz, U.row, U.col, U.val, U.c, U.rL, U.rU, U.l, U.u, U.obj_offset, 0)
+    P = O.RefProblem(h, lib)
+    # same form in, no presolve: the reference pipeline rebuilds the PDLP form and scaling
+    ref = P.solve_pdhg(max_iterations=500000, tol=1e-6)
+    assert ref["iterations"] == r["iterations"]
+    np.testing.assert_array_equal(ref["x"], r["x"])
+    np.testing.assert_array_equal(ref["y"], r["y"])
+
+
+@pytest.mark.skipif(not O.reference_available(), reason="reference library not built here")
+@pytest.mark.parametrize("name", FIX)
+def test_verify_and_scale_bitexact_with_reference(name):
+    U, S, Dr, Dc = load_fixture(name)
+    rng = np.random.default_rng(3)
+    x = rng.normal(size=U.n)
+    y = rng.normal(size=U.m)
+    lib = O.reference()
+    h = lib.ref_from_arrays(U.m, U.n, U.nnz, U.row, U.col, U.val, U.c, U.rL, U.rU, U.l, U.u, U.obj_offset, 0)
+    P = O.RefProblem(h, lib)
+    a = P.verify_form(P.ORIGINAL, x, y)
+    b = O.verify(U, x, y)
+    for k in ("eps_P", "eps_D", "eps_G", "objective"):
+        assert a[k] == b[k] or (np.isinf(a[k]) and np.isinf(b[k]))
+    s1, Dr1, Dc1 = O.scale(U)
+    s2, Dr2, Dc2 = O.ref_scale(U)
+    np.testing.assert_array_equal(s1.val, s2.val)
+    np.testing.assert_array_equal(Dr1, Dr2)
+    np.testing.assert_array_equal(Dc1, Dc2)
+    # and the fixture's stored scaling is what scale() gives
+    np.testing.assert_array_equal(s1.val, S.val)
+    np.testing.assert_array_equal(Dr1, Dr)
+
+
+@pytest.mark.parametrize("key", sorted(golden_index()["random"].keys()))
+def test_random_family_regenerates_bitexact(key):
+    """The seeded generator still produces the LP the golden results were made on."""
+    from conftest import digest
+    lp, *_ , g = random_case(key)
+    assert digest(lp) == g["digest"]
+
+
+def test_restatement_small_random_lp_matches_reference_objective():
+    key = "rand_m300_n900_k4_s7_f32"
+    lp, U, S, Dr, Dc, g = random_case(key)
+    r = O.pdlp_run(O.LPForm(U.m, U.n, U.row, U.col, U.val, U.c, U.rL, U.rU, U.l, U.u),
+                   O.LPForm(S.m, S.n, S.row, S.col, S.val, S.c, S.rL, S.rU, S.l, S.u), Dr, Dc, tol=1e-8,
+                   max_iterations=500000)
+    assert r["converged"]
+    obj = float(np.dot(U.c, r["x"]))
+    ref = g["simplex"]["objective"]
+    assert abs(obj - ref) / max(1.0, abs(ref)) < 1e-6
