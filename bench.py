@@ -38,6 +38,13 @@ WORKLOADS = {
 }
 
 
+# Attempts the reference algorithm (include/pdlp_algo.hpp) needs to reach 1e-6 on each workload,
+# used to turn the reference CPU engine's measured attempts/s into solves/s. "small" is the
+# reference's own count (tests/golden/golden.json); the others are this engine's FP64-mode
+# count, which takes the reference's decisions (tests/test_gpu_solve.py).
+REF_ATTEMPTS = {"large": 143360, "medium": 73024, "small": 13888}
+
+
 def describe(name):
     kind, p = WORKLOADS[name]
     if kind == "random":
@@ -175,9 +182,9 @@ def reference_arm(args, world, rank):
     value = 1.0 / (sec_per_attempt * attempts)
     cb = {"value": value, "unit": UNIT, "cores": 1, "kind": "reference",
           "sample": f"{args.cpu_sample_iters} attempts of solve_pdhg per step on this LP; solves/s = "
-                    f"attempts/s / {attempts} attempts per solve (the engine's count at 1e-6)"}
+                    f"attempts/s / {attempts} attempts per solve at 1e-6"}
     return {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": 1e3 * sec_per_attempt * args.cpu_sample_iters,
+            "warmup": args.warmup, "ms_per_step": 1e3 / value,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic", "impl": "reference", "config": workload_config(args, U, lp),
             "cpu_baseline": cb, "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0,
@@ -205,6 +212,24 @@ def workload_config(args, U, lp):
             "parallelism": f"replicas x{args.gpus}" if args.gpus > 1 else "single GPU"}
 
 
+def profile_mode(args):
+    """Short runs for profiler captures: builds the engine for the workload and
+    launches only the kernel under study."""
+    import b200pdlp as B
+    lp = make_lp(B, args.workload)
+    U, S, Dr, Dc, _ = B.prepare(lp)
+    prec = B.PREC_MIXED if args.precision == "mixed" else B.PREC_FP64
+    with B.Engine(U, S, Dr, Dc) as eng:
+        if args.mode == "spmv":
+            a = eng.spmv_bench(0, prec, args.reps)
+            t = eng.spmv_bench(1, prec, args.reps)
+            print(f"spmv A {a * 1e3:.1f} us, A^T {t * 1e3:.1f} us ({args.precision} vectors)")
+        else:
+            r = eng.solve(max_iterations=args.max_attempts, tol=args.tol, precision=prec, copy_out=False)
+            print(f"solve: {r.iterations} attempts, {r.stats['device_ms']:.2f} ms, "
+                  f"{1e3 * r.stats['device_ms'] / max(1, r.iterations):.1f} us/attempt")
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -220,12 +245,18 @@ def main():
                     help="attempts per solve used to turn the reference's attempts/s into solves/s "
                          "(0: take the engine's own count from a solve of this LP)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--mode", default="bench", choices=["bench", "spmv", "solve"],
+                    help="spmv / solve: one short run of that kernel for profiling (ncu), no JSON line")
+    ap.add_argument("--max-attempts", type=int, default=256, help="--mode solve: attempt limit")
+    ap.add_argument("--reps", type=int, default=1, help="--mode spmv: timed launches per product")
     args = ap.parse_args()
     world, rank, local = dist_setup(args.gpus)
+    if args.mode != "bench":
+        return profile_mode(args)
 
     if args.impl == "reference":
         if args.ref_attempts_per_solve <= 0:
-            args.ref_attempts_per_solve = 10_000
+            args.ref_attempts_per_solve = REF_ATTEMPTS.get(args.workload, 10_000)
         line = reference_arm(args, world, rank)
         if rank == 0 and line is not None:
             print(json.dumps(line), flush=True)

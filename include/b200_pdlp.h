@@ -149,6 +149,14 @@ int b2_engine_spmv(b2_engine* e, int32_t which, const double* x, double* y);
 int b2_engine_spmv_bench(b2_engine* e, int32_t which, int32_t precision, int32_t reps, void* stream,
                          double* avg_ms);
 
+/* Per-check records of the engine's last solve, B2_TRACE_FIELDS doubles each:
+ * attempts, accepted, eps_P/eps_D/eps_G of the current point, the same of the
+ * average point, primal weight, step size, flags (1 restart, 2 restart to the
+ * average, 4 FP32 iterates, 8/16 new best = current/average), weight of the
+ * average. At most max_records are copied; *count receives how many. */
+#define B2_TRACE_FIELDS 12
+int b2_engine_trace(b2_engine* e, double* out, int32_t max_records, int32_t* count);
+
 /* ---- host-side preparation (product side, no GPU needed) ---------------- */
 
 /* Ruiz (ruiz_passes) + Pock-Chambolle alpha=1 scaling, as scale() in

@@ -38,7 +38,8 @@ EXIT_CONVERGED, EXIT_MAX_ITER, EXIT_STOPPED, EXIT_TIME_LIMIT = 1, 2, 3, 4
 
 EXPORTED = [
     "b2_default_opts", "b2_solve_pdhg_gpu", "b2_solve_pdhg_gpu_ex", "b2_engine_create", "b2_engine_solve",
-    "b2_engine_destroy", "b2_engine_get_info", "b2_engine_spmv", "b2_engine_spmv_bench", "b2_scale",
+    "b2_engine_destroy", "b2_engine_get_info", "b2_engine_spmv", "b2_engine_spmv_bench", "b2_engine_trace",
+    "b2_scale",
     "b2_gen_random_lp", "b2_gen_transport", "b2_last_error", "b2_version",
 ]
 
@@ -109,6 +110,7 @@ def lib():
             L.b2_engine_get_info.argtypes = [vp, C.POINTER(EngineInfo)]
             L.b2_engine_spmv.argtypes = [vp, i32, vp, vp]
             L.b2_engine_spmv_bench.argtypes = [vp, i32, i32, i32, vp, C.POINTER(f64)]
+            L.b2_engine_trace.argtypes = [vp, vp, i32, C.POINTER(i32)]
             L.b2_scale.argtypes = [C.POINTER(_LPView), i32] + [vp] * 8
             L.b2_gen_random_lp.argtypes = [i32, i32, i32, C.c_uint64, i32] + [vp] * 8
             L.b2_gen_transport.argtypes = [i32, i32, C.c_uint64] + [vp] * 8
@@ -302,6 +304,16 @@ class Engine:
         y = np.zeros(max(rows, 1))
         _check(lib().b2_engine_spmv(self._h, which, _ptr(xx), _ptr(y)))
         return y[:rows]
+
+    TRACE_FIELDS = ("attempts", "accepted", "eps_P", "eps_D", "eps_G", "avg_eps_P", "avg_eps_D", "avg_eps_G",
+                    "omega", "eta", "flags", "avg_weight")
+
+    def trace(self, max_records: int = 65536) -> np.ndarray:
+        """Per-check records of the last solve, shape (checks, 12), columns TRACE_FIELDS."""
+        out = np.zeros((max_records, len(self.TRACE_FIELDS)))
+        n = C.c_int32()
+        _check(lib().b2_engine_trace(self._h, _ptr(out), max_records, C.byref(n)))
+        return out[:n.value]
 
     def spmv_bench(self, which: int, precision: int = PREC_MIXED, reps: int = 20, stream=None) -> float:
         ms = C.c_double()

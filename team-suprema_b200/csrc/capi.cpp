@@ -56,7 +56,7 @@ void b2_default_opts(b2_solve_opts* o) {
     o->tol = 1e-6;
     o->precision = B2_PREC_MIXED;
     o->switch_tol = 1e-5;
-    o->stall_checks = 8;
+    o->stall_checks = 32;
     o->time_limit_s = 0.0;
     o->barrier_timeout_s = 10.0;
 }
@@ -140,6 +140,13 @@ int b2_engine_spmv_bench(b2_engine* e, int32_t which, int32_t precision, int32_t
     return b2::guarded([&] {
         if (!e || !avg_ms || (which != 0 && which != 1) || reps < 0) b2::fail(B2_ERR_INVALID, "bad argument");
         b2::engine_spmv_bench(e->impl, which, precision, reps, stream, avg_ms);
+    });
+}
+
+int b2_engine_trace(b2_engine* e, double* out, int32_t max_records, int32_t* count) {
+    return b2::guarded([&] {
+        if (!e || !count) b2::fail(B2_ERR_INVALID, "null argument");
+        *count = b2::engine_trace(e->impl, out, max_records);
     });
 }
 

@@ -52,6 +52,10 @@ constexpr int kPartStride = 32;  // doubles per CTA per reduction slot
 constexpr int kMaxNV = 22;
 enum { SLOT_A = 0, SLOT_X = 1, SLOT_CK = 2, NSLOTS = 3 };
 enum { SEL_BEST = 0, SEL_CUR = 1, SEL_AVG = 2 };
+// one record per KKT check: attempts, accepted, eps_P/D/G of the current point,
+// eps_P/D/G of the average, omega, eta, flags (restart | avg<<1 | fp32<<2 |
+// best<<3), weight of the average
+constexpr int kTraceFields = 12;
 enum { MODE_START = 0, MODE_RESUME = 1 };
 constexpr double kInfD = __builtin_huge_val();
 
@@ -106,6 +110,8 @@ struct KParamsBase {
     unsigned long long timeout_ns;
     int max_iterations, check_every, stall_checks, return_current, mixed;
     unsigned long long debug_delay_ns;  // test hook: CTA 0 arrives late at its first barrier
+    double* trace;                      // per-check records (kTraceFields doubles), may be null
+    int trace_cap;
 };
 
 template <class T>
@@ -578,6 +584,15 @@ __device__ void check_decision(const KParamsBase& B, Ctl& s, const double* t, bo
     flags[0] = best_sel;
     flags[1] = restart;
     flags[2] = use_avg;
+    if (blockIdx.x == 0 && B.trace && s.checks - 1 < B.trace_cap) {
+        double* t_out = B.trace + (size_t)(s.checks - 1) * kTraceFields;
+        t_out[0] = s.attempts; t_out[1] = s.accepted;
+        t_out[2] = eP[0]; t_out[3] = eD[0]; t_out[4] = eG[0];
+        t_out[5] = eP[1]; t_out[6] = eD[1]; t_out[7] = eG[1];
+        t_out[8] = s.omega; t_out[9] = s.eta;
+        t_out[10] = restart | (use_avg << 1) | ((FP32 ? 1 : 0) << 2) | (best_sel << 3);
+        t_out[11] = *wsum_old;
+    }
 }
 
 // -------------------------------------------------------------- the kernel
@@ -898,6 +913,9 @@ struct EngineImpl {
     unsigned* bar = nullptr;
     int* abort_flag = nullptr;
     dev::Ctl* ctl = nullptr;
+    static constexpr int kTraceCap = 65536;
+    double* trace = nullptr;  // per-check records of the last solve
+    int last_checks = 0;
     int* h_stop = nullptr;   // pinned, mapped
     int* d_stop = nullptr;
     int max_ctas = 0;
@@ -975,6 +993,7 @@ struct EngineImpl {
         bar = alloc<unsigned>(1);
         abort_flag = alloc<int>(1);
         ctl = alloc<dev::Ctl>(1);
+        trace = alloc<double>((size_t)kTraceCap * dev::kTraceFields);
         // host stop word: pinned and mapped so the device can poll it
         cuda_ok(cudaHostAlloc((void**)&h_stop, sizeof(int), cudaHostAllocMapped), "cudaHostAlloc");
         *h_stop = 0;
@@ -1017,10 +1036,12 @@ struct EngineImpl {
         P.timeout_ns = (unsigned long long)((o.barrier_timeout_s > 0 ? o.barrier_timeout_s : 10.0) * 1e9);
         P.max_iterations = o.max_iterations;
         P.check_every = std::max(1, o.check_every);
-        P.stall_checks = o.stall_checks > 0 ? o.stall_checks : 8;
+        P.stall_checks = o.stall_checks > 0 ? o.stall_checks : 32;
         P.return_current = o.return_current;
         P.mixed = o.precision == B2_PREC_MIXED;
         P.debug_delay_ns = o.debug_delay_us > 0 ? (unsigned long long)o.debug_delay_us * 1000ull : 0ull;
+        P.trace = trace;
+        P.trace_cap = kTraceCap;
         return P;
     }
 
@@ -1086,6 +1107,7 @@ struct EngineImpl {
         cuda_ok(cudaEventElapsedTime(&ms, ev0, ev1), "elapsed");
         dev::Ctl fin{};
         cuda_ok(cudaMemcpy(&fin, ctl, sizeof(fin), cudaMemcpyDeviceToHost), "ctl download");
+        last_checks = fin.checks;
         if (x_out && L.n) cuda_ok(cudaMemcpy(x_out, out_x, sizeof(double) * L.n, cudaMemcpyDeviceToHost), "x download");
         if (y_out && L.m) cuda_ok(cudaMemcpy(y_out, out_y, sizeof(double) * L.m, cudaMemcpyDeviceToHost), "y download");
         if (res) {
@@ -1216,6 +1238,13 @@ void engine_info(EngineImpl* e, b2_engine_info* info) {
 }
 
 void engine_spmv(EngineImpl* e, int which, const double* x, double* y) { e->spmv(which, x, y); }
+
+int engine_trace(EngineImpl* e, double* out, int max_records) {
+    const int n = std::min(std::min(e->last_checks, EngineImpl::kTraceCap), std::max(0, max_records));
+    if (n > 0 && out)
+        cuda_ok(cudaMemcpy(out, e->trace, sizeof(double) * dev::kTraceFields * n, cudaMemcpyDeviceToHost), "trace");
+    return n;
+}
 
 void engine_spmv_bench(EngineImpl* e, int which, int precision, int reps, void* stream, double* avg_ms) {
     e->spmv_bench(which, precision, reps, stream, avg_ms);

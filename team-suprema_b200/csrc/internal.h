@@ -83,6 +83,7 @@ void engine_solve(EngineImpl* e, const b2_solve_opts& o, const volatile int32_t*
                   b2_result* r);
 void engine_info(EngineImpl* e, b2_engine_info* info);
 void engine_spmv(EngineImpl* e, int which, const double* x, double* y);
+int engine_trace(EngineImpl* e, double* out, int max_records);
 void engine_spmv_bench(EngineImpl* e, int which, int precision, int reps, void* stream, double* avg_ms);
 
 }  // namespace b2
