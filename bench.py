@@ -35,6 +35,7 @@ WORKLOADS = {
     "transport": ("transport", dict(S=2000, D=500, seed=1)),
     "small": ("random", dict(m=600, n=1800, k=6, seed=0, fp32=False)),
     "medium": ("random", dict(m=50_000, n=150_000, k=6, seed=3, fp32=True)),
+    "batch": ("batch", dict(count=4096, seed=0)),
 }
 
 
@@ -47,6 +48,9 @@ REF_ATTEMPTS = {"large": 143360, "medium": 73024, "small": 13888}
 
 def describe(name):
     kind, p = WORKLOADS[name]
+    if kind == "batch":
+        return (f"batch of {p['count']} random equality LPs, m log-uniform [50,5000], n=round(U[2,4] m), "
+                f"U{{4..10}} nnz/col, FP32 values, seed {p['seed']}")
     if kind == "random":
         return (f"random equality LP m={p['m']} n={p['n']} {p['k']} nnz/col values "
                 f"{'FP32' if p['fp32'] else 'FP64'} U[-1,1], 0<=x<=10, seed {p['seed']}")
@@ -212,6 +216,67 @@ def workload_config(args, U, lp):
             "parallelism": f"replicas x{args.gpus}" if args.gpus > 1 else "single GPU"}
 
 
+def make_batch(B, name):
+    _, p = WORKLOADS[name]
+    probs = []
+    for (m, n, k, seed) in B.batch_family_shapes(p["count"], p["seed"]):
+        lp = B.gen_random_lp(m, n, k, seed, True)
+        U, S, Dr, Dc, _ = B.prepare(lp)
+        probs.append((U, S, Dr, Dc))
+    return probs
+
+
+def batch_bench(args, world, rank, local):
+    """One step = one persistent launch solving the whole batch to 1e-6."""
+    import torch
+    import b200pdlp as B
+    torch.cuda.set_device(local)
+    prec = B.PREC_MIXED if args.precision == "mixed" else B.PREC_FP64
+    t0 = time.time()
+    probs = make_batch(B, args.workload)
+    t_prep = time.time() - t0
+    t0 = time.time()
+    bt = B.Batch(probs)
+    t_create = time.time() - t0
+    info = bt.info()
+    bopts = dict(precision=prec, batch_block=args.batch_block, batch_cluster_nnz=args.batch_cluster_nnz)
+    for _ in range(args.warmup):
+        bt.solve(max_iterations=2_000_000, tol=args.tol, **bopts)
+    dist_barrier(world)
+    steps = []
+    with ClockSampler(local) as clk:
+        for _ in range(args.steps):
+            res, ms = bt.solve(max_iterations=2_000_000, tol=args.tol, **bopts)
+            steps.append((res, ms))
+    dist_barrier(world)
+    ms_total = dist_max(sum(ms for _, ms in steps), world)
+    n_lp = len(probs)
+    value = world * n_lp * args.steps / (ms_total / 1e3)
+    res = steps[-1][0]
+    lat = sorted(r["device_ms"] for r in res)
+    conv = sum(r["converged"] for r in res)
+    attempts = np.array([r["iterations"] for r in res])
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_total / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64" if prec == B.PREC_MIXED else "f64",
+            "data": "synthetic",
+            "config": {"workload": describe(args.workload), "lps": n_lp, "sum_m": info["sum_m"],
+                       "sum_n": info["sum_n"], "sum_nnz": info["sum_nnz"], "tol": args.tol,
+                       "batch_block": bt.info()["threads_per_cta"], "batch_cluster_nnz": args.batch_cluster_nnz,
+                       "parallelism": f"replicas x{world}" if world > 1 else "single GPU"},
+            "latency_ms": {"p50": lat[len(lat) // 2], "p99": lat[int(0.99 * (len(lat) - 1))], "max": lat[-1],
+                           "note": "per-LP time on its CTA inside the launch"},
+            "converged": conv, "attempts": {"median": float(np.median(attempts)), "max": int(attempts.max()),
+                                            "total": int(attempts.sum())},
+            "clocks": clk.summary(), "gpu_launches": args.steps, "prep_s": t_prep, "create_s": t_create,
+            "device_bytes": info["device_bytes"],
+        }
+        print(json.dumps(line), flush=True)
+    bt.close()
+
+
 def profile_mode(args):
     """Short runs for profiler captures: builds the engine for the workload and
     launches only the kernel under study."""
@@ -249,10 +314,15 @@ def main():
                     help="spmv / solve: one short run of that kernel for profiling (ncu), no JSON line")
     ap.add_argument("--max-attempts", type=int, default=256, help="--mode solve: attempt limit")
     ap.add_argument("--reps", type=int, default=1, help="--mode spmv: timed launches per product")
+    ap.add_argument("--batch-block", type=int, default=0, help="batch: threads per CTA (128/256/512, 0 auto)")
+    ap.add_argument("--batch-cluster-nnz", type=int, default=0,
+                    help="batch: stored entries from which an LP is solved by a cluster (0 auto, <0 never)")
     args = ap.parse_args()
     world, rank, local = dist_setup(args.gpus)
     if args.mode != "bench":
         return profile_mode(args)
+    if WORKLOADS[args.workload][0] == "batch":
+        return batch_bench(args, world, rank, local)
 
     if args.impl == "reference":
         if args.ref_attempts_per_solve <= 0:

@@ -73,6 +73,9 @@ typedef struct b2_solve_opts {
     void* stream;             /* cudaStream_t to launch on; NULL: the engine's own stream  */
     int32_t debug_delay_us;   /* test hook: CTA 0 reaches its first barrier this late (bounded),
                                  so a short barrier_timeout_s exercises the timeout path   */
+    int32_t batch_cluster_nnz;/* batches: LPs with at least this many stored entries (A and A^T)
+                                 are solved by a cluster of 8 CTAs; <= 0: never (default)     */
+    int32_t batch_block;      /* batches: threads per CTA, 128, 256 or 512; 0: auto (512)     */
 } b2_solve_opts;
 
 void b2_default_opts(b2_solve_opts* opts);
@@ -156,6 +159,35 @@ int b2_engine_spmv_bench(b2_engine* e, int32_t which, int32_t precision, int32_t
  * average. At most max_records are copied; *count receives how many. */
 #define B2_TRACE_FIELDS 12
 int b2_engine_trace(b2_engine* e, double* out, int32_t max_records, int32_t* count);
+
+/* ---- batches: many LPs of uneven size in one persistent launch -----------
+ * No counterpart in the reference, which solves one LP per call; each LP of a
+ * batch is the same solve as b2_solve_pdhg_gpu on that LP (same inputs, same
+ * options, bit-identical answer), run by one CTA that takes the next LP from
+ * a device work queue when it finishes. unscaled[i], scaled[i], Dr[i], Dc[i]
+ * describe LP i exactly as for b2_solve_pdhg_gpu. */
+typedef struct b2_batch b2_batch;
+
+typedef struct b2_batch_info {
+    int32_t n_lp;
+    int64_t sum_m, sum_n, sum_nnz, sum_padded;
+    int32_t max_ctas, threads_per_cta;
+    int64_t device_bytes;
+} b2_batch_info;
+
+int b2_batch_create(int32_t n_lp, const b2_lp_view* unscaled, const b2_lp_view* scaled, const double* const* Dr,
+                    const double* const* Dc, const b2_solve_opts* opts, b2_batch** out);
+/* Solves every LP of the batch; results[i] receives LP i's result (device_ms =
+ * that LP's time on its CTA); *total_ms the whole launch (CUDA events). */
+int b2_batch_solve(b2_batch* b, const b2_solve_opts* opts, const volatile int32_t* stop_flag, b2_result* results,
+                   double* total_ms);
+/* Copies LP i's returned point (unscaled PDLP-form space) of the last solve. */
+int b2_batch_get_solution(b2_batch* b, int32_t i, double* x, double* y);
+int b2_batch_get_info(b2_batch* b, b2_batch_info* info);
+/* y = A x (which = 0) or A^T x (which = 1) of LP i through the batch's packed
+ * device layout (FP64 accumulation); x, y in that LP's caller order. */
+int b2_batch_spmv(b2_batch* b, int32_t i, int32_t which, const double* x, double* y);
+void b2_batch_destroy(b2_batch* b);
 
 /* ---- host-side preparation (product side, no GPU needed) ---------------- */
 

@@ -39,6 +39,8 @@ EXIT_CONVERGED, EXIT_MAX_ITER, EXIT_STOPPED, EXIT_TIME_LIMIT = 1, 2, 3, 4
 EXPORTED = [
     "b2_default_opts", "b2_solve_pdhg_gpu", "b2_solve_pdhg_gpu_ex", "b2_engine_create", "b2_engine_solve",
     "b2_engine_destroy", "b2_engine_get_info", "b2_engine_spmv", "b2_engine_spmv_bench", "b2_engine_trace",
+    "b2_batch_create", "b2_batch_solve", "b2_batch_get_solution", "b2_batch_get_info", "b2_batch_spmv",
+    "b2_batch_destroy",
     "b2_scale",
     "b2_gen_random_lp", "b2_gen_transport", "b2_last_error", "b2_version",
 ]
@@ -64,7 +66,8 @@ class SolveOpts(C.Structure):
                 ("precision", C.c_int32), ("switch_tol", C.c_double), ("stall_checks", C.c_int32),
                 ("time_limit_s", C.c_double), ("barrier_timeout_s", C.c_double), ("max_ctas", C.c_int32),
                 ("lane_target", C.c_int32), ("sigma_window", C.c_int32), ("return_current", C.c_int32),
-                ("stream", C.c_void_p), ("debug_delay_us", C.c_int32)]
+                ("stream", C.c_void_p), ("debug_delay_us", C.c_int32), ("batch_cluster_nnz", C.c_int32),
+                ("batch_block", C.c_int32)]
 
 
 class _Result(C.Structure):
@@ -73,6 +76,12 @@ class _Result(C.Structure):
                 ("objective", C.c_double), ("exit_reason", C.c_int32), ("checks", C.c_int32),
                 ("fp32_attempts", C.c_int32), ("fp32_accepted", C.c_int32), ("device_ms", C.c_double),
                 ("host_ms", C.c_double), ("final_eta", C.c_double), ("final_omega", C.c_double)]
+
+
+class BatchInfo(C.Structure):
+    _fields_ = [("n_lp", C.c_int32), ("sum_m", C.c_int64), ("sum_n", C.c_int64), ("sum_nnz", C.c_int64),
+                ("sum_padded", C.c_int64), ("max_ctas", C.c_int32), ("threads_per_cta", C.c_int32),
+                ("device_bytes", C.c_int64)]
 
 
 class EngineInfo(C.Structure):
@@ -111,6 +120,14 @@ def lib():
             L.b2_engine_spmv.argtypes = [vp, i32, vp, vp]
             L.b2_engine_spmv_bench.argtypes = [vp, i32, i32, i32, vp, C.POINTER(f64)]
             L.b2_engine_trace.argtypes = [vp, vp, i32, C.POINTER(i32)]
+            L.b2_batch_create.argtypes = [i32, C.POINTER(_LPView), C.POINTER(_LPView), C.POINTER(vp), C.POINTER(vp),
+                                          C.POINTER(SolveOpts), C.POINTER(vp)]
+            L.b2_batch_solve.argtypes = [vp, C.POINTER(SolveOpts), vp, C.POINTER(_Result), C.POINTER(f64)]
+            L.b2_batch_get_solution.argtypes = [vp, i32, vp, vp]
+            L.b2_batch_get_info.argtypes = [vp, C.POINTER(BatchInfo)]
+            L.b2_batch_spmv.argtypes = [vp, i32, i32, vp, vp]
+            L.b2_batch_destroy.argtypes = [vp]
+            L.b2_batch_destroy.restype = None
             L.b2_scale.argtypes = [C.POINTER(_LPView), i32] + [vp] * 8
             L.b2_gen_random_lp.argtypes = [i32, i32, i32, C.c_uint64, i32] + [vp] * 8
             L.b2_gen_transport.argtypes = [i32, i32, C.c_uint64] + [vp] * 8
@@ -321,6 +338,96 @@ class Engine:
         return ms.value
 
 
+class Batch:
+    """Many LPs in one persistent launch (b2_batch_*): one CTA per LP, a device
+    work queue, retired LPs hand their CTA to the next. problems is a list of
+    (unscaled_form, scaled_form, Dr, Dc) tuples, each exactly what
+    solve_pdhg_gpu takes; LP i's answer equals solve_pdhg_gpu on LP i."""
+
+    def __init__(self, problems, **opts):
+        self.n = len(problems)
+        self._keep = []
+        U_arr = (_LPView * self.n)()
+        S_arr = (_LPView * self.n)()
+        dr_arr = (C.c_void_p * self.n)()
+        dc_arr = (C.c_void_p * self.n)()
+        self.dims = []
+        for i, (U, S, Dr, Dc) in enumerate(problems):
+            U = RangedLP.like(U)
+            S = RangedLP.like(S)
+            Dr = _vec(Dr, U.m)
+            Dc = _vec(Dc, U.n)
+            if Dr.size == 0:
+                Dr = np.zeros(1)
+            if Dc.size == 0:
+                Dc = np.zeros(1)
+            self._keep += [U, S, Dr, Dc]
+            U_arr[i] = U.view()
+            S_arr[i] = S.view()
+            dr_arr[i] = _ptr(Dr)
+            dc_arr[i] = _ptr(Dc)
+            self.dims.append((U.m, U.n))
+        o = default_opts(**opts)
+        h = C.c_void_p()
+        _check(lib().b2_batch_create(self.n, U_arr, S_arr, dr_arr, dc_arr, C.byref(o), C.byref(h)))
+        self._h = h
+        self._keep = []  # the engine holds its own copy of the data
+
+    def close(self):
+        if getattr(self, "_h", None) and self._h.value:
+            lib().b2_batch_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def solve(self, max_iterations: int = 200000, check_every: int = 64, tol: float = 1e-6,
+              stop_flag: Optional[StopFlag] = None, **opts):
+        """Returns (list of per-LP stats dicts, total device ms of the launch)."""
+        o = default_opts(max_iterations=int(max_iterations), check_every=int(check_every), tol=float(tol), **opts)
+        res = (_Result * self.n)()
+        ms = C.c_double()
+        _check(lib().b2_batch_solve(self._h, C.byref(o), stop_flag.ptr if stop_flag else None, res, C.byref(ms)))
+        out = []
+        for r in res:
+            d = {k: getattr(r, k) for k, _ in _Result._fields_}
+            d["converged"] = bool(d["converged"])
+            out.append(d)
+        return out, ms.value
+
+    def solution(self, i: int):
+        m, n = self.dims[i]
+        x = np.zeros(max(n, 1))
+        y = np.zeros(max(m, 1))
+        _check(lib().b2_batch_get_solution(self._h, i, _ptr(x), _ptr(y)))
+        return x[:n], y[:m]
+
+    def spmv(self, i: int, which: int, x) -> np.ndarray:
+        """A x (which=0) or A^T x (which=1) of LP i through the packed device layout."""
+        m, n = self.dims[i]
+        rows, cols = (m, n) if which == 0 else (n, m)
+        xx = _vec(x, cols)
+        if xx.size == 0:
+            xx = np.zeros(1)
+        y = np.zeros(max(rows, 1))
+        _check(lib().b2_batch_spmv(self._h, i, which, _ptr(xx), _ptr(y)))
+        return y[:rows]
+
+    def info(self) -> dict:
+        i = BatchInfo()
+        _check(lib().b2_batch_get_info(self._h, C.byref(i)))
+        return {k: getattr(i, k) for k, _ in BatchInfo._fields_}
+
+
 # ------------------------------------------------------------- host-side prep
 def scale(lp: RangedLP, ruiz_passes: int = 10):
     """Ruiz + Pock-Chambolle scaling (src/scaling.cpp:25-84). Returns (scaled, Dr, Dc)."""
@@ -388,6 +495,18 @@ def gen_random_lp(m: int, n: int, k: int, seed: int = 0, fp32_values: bool = Fal
     _check(lib().b2_gen_random_lp(m, n, k, seed, int(fp32_values), *[_ptr(a) for a in (row, col, val, c, rL, rU,
                                                                                        l, u)]))
     return RangedLP(m, n, row, col, val, c, rL, rU, l, u)
+
+
+def batch_family_shapes(count: int, seed: int = 0, m_lo: int = 50, m_hi: int = 5000):
+    """Shapes of the uneven batch family: m log-uniform on [m_lo, m_hi],
+    n = round(U[2,4] m), nonzeros per column uniform on {4..10}; one derived
+    seed per LP. Returns a list of (m, n, k, seed)."""
+    rng = np.random.default_rng(seed)
+    m = np.exp(rng.uniform(np.log(m_lo), np.log(m_hi), count)).round().astype(int)
+    n = np.round(rng.uniform(2.0, 4.0, count) * m).astype(int)
+    k = rng.integers(4, 11, count)
+    seeds = rng.integers(0, 2**62, count)
+    return [(int(a), int(b), int(c), int(d)) for a, b, c, d in zip(m, n, k, seeds)]
 
 
 def gen_transport(S: int, D: int, seed: int = 0) -> RangedLP:

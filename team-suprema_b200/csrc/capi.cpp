@@ -47,6 +47,10 @@ struct b2_engine {
     b2::EngineImpl* impl;
 };
 
+struct b2_batch {
+    b2::BatchImpl* impl;
+};
+
 extern "C" {
 
 void b2_default_opts(b2_solve_opts* o) {
@@ -148,6 +152,54 @@ int b2_engine_trace(b2_engine* e, double* out, int32_t max_records, int32_t* cou
         if (!e || !count) b2::fail(B2_ERR_INVALID, "null argument");
         *count = b2::engine_trace(e->impl, out, max_records);
     });
+}
+
+int b2_batch_create(int32_t n_lp, const b2_lp_view* U, const b2_lp_view* S, const double* const* Dr,
+                    const double* const* Dc, const b2_solve_opts* opts, b2_batch** out) {
+    return b2::guarded([&] {
+        if (!U || !S || !Dr || !Dc || !out) b2::fail(B2_ERR_INVALID, "null argument");
+        b2_solve_opts o;
+        if (opts) o = *opts;
+        else b2_default_opts(&o);
+        *out = nullptr;
+        b2::BatchImpl* b = b2::batch_create(n_lp, U, S, Dr, Dc, o);
+        *out = new b2_batch{b};
+    });
+}
+
+int b2_batch_solve(b2_batch* b, const b2_solve_opts* opts, const volatile int32_t* stop_flag, b2_result* results,
+                   double* total_ms) {
+    return b2::guarded([&] {
+        if (!b || !opts) b2::fail(B2_ERR_INVALID, "null argument");
+        b2::batch_solve(b->impl, *opts, stop_flag, results, total_ms);
+    });
+}
+
+int b2_batch_get_solution(b2_batch* b, int32_t i, double* x, double* y) {
+    return b2::guarded([&] {
+        if (!b) b2::fail(B2_ERR_INVALID, "null argument");
+        b2::batch_solution(b->impl, i, x, y);
+    });
+}
+
+int b2_batch_get_info(b2_batch* b, b2_batch_info* info) {
+    return b2::guarded([&] {
+        if (!b || !info) b2::fail(B2_ERR_INVALID, "null argument");
+        b2::batch_info(b->impl, info);
+    });
+}
+
+int b2_batch_spmv(b2_batch* b, int32_t i, int32_t which, const double* x, double* y) {
+    return b2::guarded([&] {
+        if (!b || !x || !y || (which != 0 && which != 1)) b2::fail(B2_ERR_INVALID, "bad argument");
+        b2::batch_spmv(b->impl, i, which, x, y);
+    });
+}
+
+void b2_batch_destroy(b2_batch* b) {
+    if (!b) return;
+    b2::batch_destroy(b->impl);
+    delete b;
 }
 
 int b2_scale(const b2_lp_view* lp, int32_t ruiz_passes, double* val_s, double* c_s, double* rL_s, double* rU_s,

@@ -1,0 +1,912 @@
+// device.cuh -- device side of the B200 PDLP engine: the restarted PDHG loop
+// of include/pdlp_algo.hpp:49-185 as one device function, solve_body<GK, T, V>,
+// run by a "group" of CTAs that cooperate on one LP:
+//   * the whole grid of a cooperative launch for one large LP (engine.cu), its
+//     barriers a bounded software grid barrier;
+//   * a thread-block cluster per large LP in the batched kernel (batch.cu), its
+//     barriers the hardware cluster barrier;
+//   * a single CTA per small LP in the batched kernel, its barriers
+//     __syncthreads.
+//
+// Design (what replaces the reference's gpu/pdlp_gpu_solve.cu):
+//   * The reference launches 6+ kernels per attempt and makes one blocking
+//     D2H copy per attempt for the step-size test (pdlp_gpu_solve.cu:232-243),
+//     plus 4 full-vector D2H copies and 2 host verify() calls every 64
+//     accepted steps (pdlp_algo.hpp:135-141). Here nothing leaves the device
+//     until the solve ends: every CTA keeps a replica of the scalar control
+//     state and takes identical decisions from identical, fixed-order sums.
+//   * Two fused passes per attempt, separated by a group barrier:
+//       rows: A x' (sliced ELL) + dual step + projection + |dy|^2, dy'(Ax'-Ax)
+//             + the deferred ergodic-average update of y;
+//       cols: [if accepted] A^T y' + the average update of x, then the primal
+//             step + bound projection for the NEXT attempt + |dx|^2.
+//   * The KKT check (verify.cpp:24-103 on the unscaled form) runs on the
+//     device: A x and A^T y of the current point are carried with the
+//     iterates, the average point takes one extra SpMV each way.
+//   * Iterates live in unscaled coordinates (x_u = Dc x_s, y_u = Dr y_s), so
+//     the matrix is stored with its ORIGINAL values (exact in FP32 for the
+//     benchmark LPs) and Ruiz / Pock-Chambolle scaling becomes the diagonal
+//     step weights tau Dc^2 and sigma Dr^2; the iteration is the reference's,
+//     in a change of variables.
+//   * Mixed precision: FP32 iterates and FP32-accumulated SpMV until the KKT
+//     error reaches switch_tol, then FP64 iterates (same control state) until
+//     `tol`. Reductions, step sizes, primal weight and KKT norms are FP64.
+//   * Every device-side wait (the grid barrier) is bounded by a wall-clock
+//     timeout; on expiry the kernel sets an abort flag, all CTAs leave, and the
+//     host reports B2_ERR_TIMEOUT with the context intact.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "internal.h"
+
+namespace b2 {
+namespace dev {
+
+constexpr int kBlock = 512;          // CTA size of the one-LP kernels (and the largest CTA size)
+constexpr int kWarps = kBlock / 32;
+constexpr int kPartStride = 32;  // doubles per CTA per reduction slot
+constexpr int kMaxNV = 22;
+enum { SLOT_A = 0, SLOT_X = 1, SLOT_CK = 2, NSLOTS = 3 };
+enum { SEL_BEST = 0, SEL_CUR = 1, SEL_AVG = 2 };
+enum { MODE_START = 0, MODE_RESUME = 1 };
+// Group kinds: one CTA (barrier __syncthreads, partial sums in shared memory,
+// iterates read through L1), a thread-block cluster (hardware cluster
+// barrier), the whole grid of a cooperative launch (software grid barrier).
+// Across SMs, iterates and partial sums go through L2 (ld.global.cg). Every
+// barrier, of every kind, is preceded by a gpu-scope fence.
+enum { GK_CTA = 0, GK_CLUSTER = 1, GK_GRID = 2 };
+// one record per KKT check: attempts, accepted, eps_P/D/G of the current point,
+// eps_P/D/G of the average, omega, eta, flags (restart | avg<<1 | fp32<<2 |
+// best<<3), weight of the average
+constexpr int kTraceFields = 12;
+constexpr double kInfD = __builtin_huge_val();
+
+struct SellDev {
+    int n_rows;
+    int n_slices;
+    const int4* slice;
+    const uint32_t* col;
+    const float* v32;
+    const double* v64;
+};
+
+template <class T>
+struct Bufs {
+    T* x[2];
+    T* y[2];
+    T* ax[3];
+    T* aty[2];
+    T* x_last;
+    T* y_last;
+};
+
+// Scalar state of pdlp_run (include/pdlp_algo.hpp:67-102), replicated per CTA.
+struct Ctl {
+    double eta, omega, wsum, pend_x, pend_y;
+    double merit_last_restart, merit_prev_cand, best_merit;
+    double best_eps[3], out_eps[3];
+    double t_start;
+    int attempts, accepted, since_restart, restarts, checks;
+    int xi, yi, ax_cur, ax_nxt, ax_avg, aty_cur, aty_avg;
+    int last_accepted, best_valid, stall, exit_reason, out_sel;
+    int mode, check_now, switch_req, stop_req;
+    int fp32_attempts, fp32_accepted;
+};
+
+// Pointers and constants of one LP (independent of the iterate precision).
+struct KParamsBase {
+    int m, n;
+    SellDev A, AT;
+    const double *b, *rU, *c, *l, *u, *x0;
+    const double *dr2, *dc2;  // Dr^2 (negated on >= rows), Dc^2
+    Bufs<float> itf;          // FP32 iterates (read when resuming in FP64)
+    double *xsum, *ysum, *best_x, *best_y, *out_x, *out_y;
+    const int32_t *perm_r, *perm_c;
+    Ctl* ctl;
+    const volatile int* host_stop;
+    double tol, switch_tol, denom_p, denom_d, time_limit_ns;
+    int max_iterations, check_every, stall_checks, return_current, mixed;
+    unsigned long long debug_delay_ns;  // test hook: the group's first CTA arrives late at its first barrier
+    double* trace;                      // per-check records (kTraceFields doubles), may be null
+    int trace_cap;
+};
+
+template <class T>
+struct KParams : KParamsBase {
+    Bufs<T> it;  // iterates at this precision
+};
+
+// The CTAs that cooperate on one LP, and this CTA's place in them.
+struct Group {
+    int rank, size;          // this CTA's index, number of CTAs
+    int gw, nw, gt, nt;      // warp / thread index and count over the group
+    double* part;            // partial sums: [NSLOTS][size][kPartStride]
+    double* bcast;           // [0] stop, [1] time limit hit, [2] start time
+    unsigned* bar;           // grid-barrier word (GK_GRID)
+    int* abort;
+    unsigned long long timeout_ns;
+    double* spart;           // GK_CTA: partial sums in shared memory, [NSLOTS][kPartStride]
+};
+
+// ------------------------------------------------------------- primitives
+__device__ __forceinline__ unsigned long long gtimer() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+// Matrix streams: read-only for the kernel's lifetime, used once per pass.
+__device__ __forceinline__ uint32_t ld_mat(const uint32_t* p) {
+    uint32_t v;
+    asm("ld.global.nc.L1::no_allocate.u32 %0, [%1];" : "=r"(v) : "l"(p));
+    return v;
+}
+__device__ __forceinline__ float ld_mat(const float* p) {
+    float v;
+    asm("ld.global.nc.L1::no_allocate.f32 %0, [%1];" : "=f"(v) : "l"(p));
+    return v;
+}
+__device__ __forceinline__ double ld_mat(const double* p) {
+    double v;
+    asm("ld.global.nc.L1::no_allocate.f64 %0, [%1];" : "=d"(v) : "l"(p));
+    return v;
+}
+// Iterates are rewritten between passes, never read through the non-coherent
+// path: inside one CTA a plain load (L1 holds the CTA's own stores), across
+// SMs a load at L2.
+template <int GK, class T>
+__device__ __forceinline__ T ld_it(const T* p) {
+    if (GK == GK_CTA) return *p;
+    return __ldcg(p);
+}
+
+template <class V>
+__device__ __forceinline__ const V* vals(const SellDev& S);
+template <>
+__device__ __forceinline__ const float* vals<float>(const SellDev& S) { return S.v32; }
+template <>
+__device__ __forceinline__ const double* vals<double>(const SellDev& S) { return S.v64; }
+
+// Sum over a warp, fixed tree; the result is taken from lane 0 and
+// broadcast, so every lane (and every CTA) sees the same bits.
+__device__ __forceinline__ double warp_total(double v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    return __shfl_sync(0xffffffffu, v, 0);
+}
+
+// Group barrier. One CTA: __syncthreads. A cluster: fence + hardware cluster
+// barrier. The grid of a cooperative launch: fence + one counter word; CTA 0
+// adds 2^31 - (N-1), the others add 1, so the top bit flips exactly when the
+// last CTA arrives. Arrival is a release, polling an acquire (gpu scope). The
+// grid wait is bounded: past timeout_ns the CTA raises `abort` and every CTA
+// leaves.
+template <int GK>
+__device__ __forceinline__ bool group_sync(const Group& g) {
+    // Make this thread's stores visible at gpu scope before anyone crosses the
+    // barrier. Needed even inside one CTA: in testing on B200, iterates read
+    // after a bare __syncthreads (plain or L2 loads) were sometimes the values
+    // from before the other threads' stores, and the solve diverged.
+    __threadfence();
+    if (GK == GK_CTA) {
+        __syncthreads();
+        return true;
+    }
+    if (GK == GK_CLUSTER) {
+        asm volatile("barrier.cluster.arrive.release.aligned;\n\tbarrier.cluster.wait.acquire.aligned;" ::: "memory");
+        return true;
+    }
+    __shared__ int s_ok;
+    __syncthreads();
+    if (g.size == 1) return true;
+    if (threadIdx.x == 0) {
+        int ok = 1;
+        const unsigned add = g.rank == 0 ? (0x80000000u - (unsigned)(g.size - 1)) : 1u;
+        unsigned old;
+        asm volatile("atom.add.release.gpu.u32 %0,[%1],%2;" : "=r"(old) : "l"(g.bar), "r"(add) : "memory");
+        const unsigned long long t0 = gtimer();
+        unsigned spins = 0;
+        for (;;) {
+            unsigned cur;
+            asm volatile("ld.acquire.gpu.u32 %0,[%1];" : "=r"(cur) : "l"(g.bar) : "memory");
+            if ((old ^ cur) & 0x80000000u) break;
+            if ((++spins & 15u) == 0) {
+                if (*(volatile int*)g.abort) { ok = 0; break; }
+                if (gtimer() - t0 > g.timeout_ns) { atomicExch(g.abort, 1); ok = 0; break; }
+            }
+        }
+        if (ok && *(volatile int*)g.abort) ok = 0;
+        s_ok = ok;
+    }
+    __syncthreads();
+    return s_ok != 0;
+}
+
+// Per-CTA partial sums of NV values: k = 0..NV-1 go to index at + k of this
+// CTA's row of the slot. Fixed order: warp tree, then warps in order.
+template <int NV, int GK>
+__device__ __forceinline__ void cta_partial_at(double (&v)[NV], const Group& g, int slot, int at, double* s_red) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+    for (int k = 0; k < NV; ++k) {
+        double t = v[k];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) t += __shfl_down_sync(0xffffffffu, t, o);
+        if (lane == 0) s_red[warp * NV + k] = t;
+    }
+    __syncthreads();
+    if (threadIdx.x < NV) {
+        double s = 0.0;
+        const int nwarps = blockDim.x >> 5;
+        for (int w = 0; w < nwarps; ++w) s += s_red[w * NV + threadIdx.x];
+        if (GK == GK_CTA) g.spart[slot * kPartStride + at + threadIdx.x] = s;
+        else g.part[((size_t)slot * g.size + g.rank) * kPartStride + at + threadIdx.x] = s;
+    }
+}
+
+template <int NV, int GK>
+__device__ __forceinline__ void cta_partial(double (&v)[NV], const Group& g, int slot, double* s_red) {
+    cta_partial_at<NV, GK>(v, g, slot, 0, s_red);
+}
+
+// After a barrier: every CTA sums the CTA partials of one slot in CTA order.
+template <int NV, int GK>
+__device__ __forceinline__ void group_totals(const Group& g, int slot, double* s_tot) {
+    if (GK == GK_CTA) {
+        if (threadIdx.x < NV) s_tot[threadIdx.x] = g.spart[slot * kPartStride + threadIdx.x];
+        __syncthreads();
+        return;
+    }
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    for (int k = warp; k < NV; k += (int)(blockDim.x >> 5)) {
+        double s = 0.0;
+        for (int b = lane; b < g.size; b += 32) s += __ldcg(&g.part[((size_t)slot * g.size + b) * kPartStride + k]);
+        s = warp_total(s);
+        if (lane == 0) s_tot[k] = s;
+    }
+    __syncthreads();
+}
+
+// Totals of the step-size statistics after a barrier: dy2 and dy'(Ax'-Ax)
+// from the rows pass, |dx|^2 from the columns pass before it.
+template <int GK>
+__device__ __forceinline__ void step_totals(const Group& g, double* s_tot) {
+    if (GK == GK_CTA) {
+        if (threadIdx.x < 3)
+            s_tot[threadIdx.x] = g.spart[(threadIdx.x < 2 ? SLOT_A : SLOT_X) * kPartStride + (threadIdx.x < 2 ? threadIdx.x : 0)];
+        __syncthreads();
+        return;
+    }
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    if (warp < 3) {
+        const int slot = warp < 2 ? SLOT_A : SLOT_X, k = warp < 2 ? warp : 0;
+        double s = 0.0;
+        for (int b = lane; b < g.size; b += 32) s += __ldcg(&g.part[((size_t)slot * g.size + b) * kPartStride + k]);
+        s = warp_total(s);
+        if (lane == 0) s_tot[warp] = s;
+    }
+    __syncthreads();
+}
+
+// One slice of a sliced-ELL matrix times a gathered vector: every lane sums
+// its share of its row in a fixed order, then the g lanes of a row are
+// folded onto the row's first lane (fixed tree).
+template <int GK, class AccT, class V, class XT>
+__device__ __forceinline__ AccT slice_dot(const SellDev& S, const V* vbase, int4 sl, int lane, const XT* x) {
+    const uint32_t len = (uint32_t)sl.y & kLenMask;
+    const int lg = (int)((uint32_t)sl.y >> kLenBits);
+    const size_t base = (size_t)(uint32_t)sl.z * 32u + (size_t)lane;
+    const uint32_t* cp = S.col + base;
+    const V* vp = vbase + base;
+    AccT acc = AccT(0);
+    uint32_t k = 0;
+    for (; k + 4 <= len; k += 4) {
+        const uint32_t c0 = ld_mat(cp), c1 = ld_mat(cp + 32), c2 = ld_mat(cp + 64), c3 = ld_mat(cp + 96);
+        const V v0 = ld_mat(vp), v1 = ld_mat(vp + 32), v2 = ld_mat(vp + 64), v3 = ld_mat(vp + 96);
+        const AccT x0 = (AccT)ld_it<GK>(x + c0), x1 = (AccT)ld_it<GK>(x + c1), x2 = (AccT)ld_it<GK>(x + c2),
+                   x3 = (AccT)ld_it<GK>(x + c3);
+        acc = fma((AccT)v0, x0, acc);
+        acc = fma((AccT)v1, x1, acc);
+        acc = fma((AccT)v2, x2, acc);
+        acc = fma((AccT)v3, x3, acc);
+        cp += 128;
+        vp += 128;
+    }
+    for (; k < len; ++k) {
+        acc = fma((AccT)ld_mat(vp), (AccT)ld_it<GK>(x + ld_mat(cp)), acc);
+        cp += 32;
+        vp += 32;
+    }
+    for (int o = (1 << lg) >> 1; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
+    return acc;
+}
+
+// verify.cpp:35-87 terms of one row: row violation^2, sign violation^2,
+// dual-objective share, -inf flag.
+__device__ __forceinline__ void kkt_row(double rl, double ru, double a, double y, double* v) {
+    const double rv = fmax(rl - a, 0.0) + fmax(a - ru, 0.0);
+    double sv = 0.0;
+    if (!isfinite(rl) && y > 0) sv += y;
+    if (!isfinite(ru) && y < 0) sv += -y;
+    double yd = y;
+    if (!isfinite(rl) && yd > 0) yd = 0.0;
+    if (!isfinite(ru) && yd < 0) yd = 0.0;
+    const double yp = fmax(yd, 0.0), yn = fmax(-yd, 0.0);
+    double d = 0.0, ninf = 0.0;
+    if (yp > 0 && isfinite(rl)) d += rl * yp;
+    if (yn > 0 && isfinite(ru)) d += -ru * yn;
+    if ((yp > 0 && !isfinite(rl)) || (yn > 0 && !isfinite(ru))) ninf = 1.0;
+    v[0] += rv * rv;
+    v[1] += sv * sv;
+    v[2] += d;
+    v[3] += ninf;
+}
+
+// The same for one column with reduced cost z = c - A^T y, plus c x.
+__device__ __forceinline__ void kkt_col(double l, double u, double cc, double x, double z, double* v) {
+    const double bv = fmax(l - x, 0.0) + fmax(x - u, 0.0);
+    double sv = 0.0;
+    if (!isfinite(l) && z > 0) sv += z;
+    if (!isfinite(u) && z < 0) sv += -z;
+    double zd = z;
+    if (!isfinite(l) && zd > 0) zd = 0.0;
+    if (!isfinite(u) && zd < 0) zd = 0.0;
+    const double zp = fmax(zd, 0.0), zn = fmax(-zd, 0.0);
+    double d = 0.0, ninf = 0.0;
+    if (zp > 0 && isfinite(l)) d += l * zp;
+    if (zn > 0 && isfinite(u)) d += -u * zn;
+    if ((zp > 0 && !isfinite(l)) || (zn > 0 && !isfinite(u))) ninf = 1.0;
+    v[0] += bv * bv;
+    v[1] += sv * sv;
+    v[2] += d;
+    v[3] += ninf;
+    v[4] += cc * x;
+}
+
+// Primal step of one column (pdlp_algo.hpp:110 / src/pdlp.cpp:122-124) in
+// unscaled coordinates: x' = clamp(x - tau Dc^2 (c - A^T y), l, u).
+template <class T>
+__device__ __forceinline__ void primal_col(const KParams<T>& P, int j, T xv, double g, double tau, T* xn,
+                                           double& dx2) {
+    const double w = __ldg(P.dc2 + j);
+    double v = (double)xv - tau * w * (__ldg(P.c + j) - g);
+    v = fmin(fmax(v, __ldg(P.l + j)), __ldg(P.u + j));
+    const T vt = (T)v;
+    xn[j] = vt;
+    const double d = (double)vt - (double)xv;
+    dx2 += d * d / w;
+}
+
+// --------------------------------------------------------------- passes
+
+// Rows: A x' fused with the dual step (pdlp_algo.hpp:111-112, src/pdlp.cpp:125-130)
+// and the step-size statistics (pdlp_gpu_solve.cu:119-131).
+template <int GK, class T, class V>
+__device__ void pass_rows_step(const KParams<T>& P, const Ctl& c, const Group& g, int lane, double* v) {
+    const T* xn = P.it.x[1 - c.xi];
+    const T* y = P.it.y[c.yi];
+    T* yn = P.it.y[1 - c.yi];
+    const T* ax = P.it.ax[c.ax_cur];
+    T* axn = P.it.ax[c.ax_nxt];
+    const double sigma = c.eta * c.omega, pend = c.pend_y;
+    const V* vb = vals<V>(P.A);
+    for (int s = g.gw; s < P.A.n_slices; s += g.nw) {
+        const int4 sl = __ldg(P.A.slice + s);
+        const T acc = slice_dot<GK, T, V, T>(P.A, vb, sl, lane, xn);
+        const int lg = (int)((uint32_t)sl.y >> kLenBits);
+        const int row = sl.x + (lane >> lg);
+        if ((lane & ((1 << lg) - 1)) == 0 && row < P.m) {
+            const T yv = ld_it<GK>(y + row), axv = ld_it<GK>(ax + row);
+            const double w = __ldg(P.dr2 + row);
+            const double aw = fabs(w);
+            double nv = (double)yv + sigma * aw * (__ldg(P.b + row) - (2.0 * (double)acc - (double)axv));
+            if (w < 0.0 && nv < 0.0) nv = 0.0;
+            const T nt = (T)nv;
+            yn[row] = nt;
+            axn[row] = acc;
+            const double d = (double)nt - (double)yv;
+            v[0] += d * d / aw;
+            v[1] += d * ((double)acc - (double)axv);
+            if (pend != 0.0) P.ysum[row] += pend * (double)yv;
+        }
+    }
+}
+
+// Columns: [accepted] A^T y' + x-average update, then the next primal step.
+template <int GK, class T, class V>
+__device__ void pass_cols_step(const KParams<T>& P, const Ctl& c, const Group& g, int lane, double& dx2) {
+    const T* x = P.it.x[c.xi];
+    T* xn = P.it.x[1 - c.xi];
+    T* aty = P.it.aty[c.aty_cur];
+    const double tau = c.eta / c.omega, pend = c.pend_x;
+    if (c.last_accepted) {
+        const T* y = P.it.y[c.yi];
+        const V* vb = vals<V>(P.AT);
+        for (int s = g.gw; s < P.AT.n_slices; s += g.nw) {
+            const int4 sl = __ldg(P.AT.slice + s);
+            const T acc = slice_dot<GK, T, V, T>(P.AT, vb, sl, lane, y);
+            const int lg = (int)((uint32_t)sl.y >> kLenBits);
+            const int j = sl.x + (lane >> lg);
+            if ((lane & ((1 << lg) - 1)) == 0 && j < P.n) {
+                aty[j] = acc;
+                const T xv = ld_it<GK>(x + j);
+                if (pend != 0.0) P.xsum[j] += pend * (double)xv;
+                primal_col<T>(P, j, xv, (double)acc, tau, xn, dx2);
+            }
+        }
+    } else {
+        for (int j = g.gt; j < P.n; j += g.nt)
+            primal_col<T>(P, j, ld_it<GK>(x + j), (double)ld_it<GK>(aty + j), tau, xn, dx2);
+    }
+}
+
+// KKT check, rows (verify.cpp:35-87 row terms) for the current and average
+// points, the average's A x, the restart distance of y, and the pending
+// y-average update.
+template <int GK, class T, class V>
+__device__ void pass_rows_check(const KParams<T>& P, const Ctl& c, const Group& g, int lane, double* v) {
+    const T* y = P.it.y[c.yi];
+    const T* ax = P.it.ax[c.ax_cur];
+    T* axa = P.it.ax[c.ax_avg];
+    const bool has_avg = c.wsum > 0;
+    const double wsum = c.wsum, pend = c.pend_y;
+    const V* vb = vals<V>(P.A);
+    for (int s = g.gw; s < P.A.n_slices; s += g.nw) {
+        const int4 sl = __ldg(P.A.slice + s);
+        double acc = 0.0;
+        if (has_avg) acc = slice_dot<GK, double, V, double>(P.A, vb, sl, lane, P.xsum);
+        const int lg = (int)((uint32_t)sl.y >> kLenBits);
+        const int i = sl.x + (lane >> lg);
+        if ((lane & ((1 << lg) - 1)) == 0 && i < P.m) {
+            const double yc = (double)ld_it<GK>(y + i);
+            double ys = __ldcg(P.ysum + i);
+            if (pend != 0.0) { ys += pend * yc; P.ysum[i] = ys; }
+            const double ac = (double)ld_it<GK>(ax + i);
+            const double aa = has_avg ? acc / wsum : ac;
+            const double ya = has_avg ? ys / wsum : yc;
+            axa[i] = (T)aa;
+            const double rl = __ldg(P.b + i), ru = __ldg(P.rU + i);
+            kkt_row(rl, ru, ac, yc, v + 0);
+            kkt_row(rl, ru, aa, ya, v + 4);
+            const double w = fabs(__ldg(P.dr2 + i)), yl = (double)ld_it<GK>(P.it.y_last + i);
+            v[8] += (yc - yl) * (yc - yl) / w;
+            v[9] += (ya - yl) * (ya - yl) / w;
+        }
+    }
+}
+
+template <int GK, class T, class V>
+__device__ void pass_cols_check(const KParams<T>& P, const Ctl& c, const Group& g, int lane, double* v) {
+    const T* x = P.it.x[c.xi];
+    const T* aty = P.it.aty[c.aty_cur];
+    T* atya = P.it.aty[c.aty_avg];
+    const bool has_avg = c.wsum > 0;
+    const double wsum = c.wsum;
+    const V* vb = vals<V>(P.AT);
+    for (int s = g.gw; s < P.AT.n_slices; s += g.nw) {
+        const int4 sl = __ldg(P.AT.slice + s);
+        double acc = 0.0;
+        if (has_avg) acc = slice_dot<GK, double, V, double>(P.AT, vb, sl, lane, P.ysum);
+        const int lg = (int)((uint32_t)sl.y >> kLenBits);
+        const int j = sl.x + (lane >> lg);
+        if ((lane & ((1 << lg) - 1)) == 0 && j < P.n) {
+            const double xc = (double)ld_it<GK>(x + j), gc = (double)ld_it<GK>(aty + j);
+            const double xa = has_avg ? __ldcg(P.xsum + j) / wsum : xc;
+            const double ga = has_avg ? acc / wsum : gc;
+            atya[j] = (T)ga;
+            const double cc = __ldg(P.c + j), l = __ldg(P.l + j), u = __ldg(P.u + j);
+            kkt_col(l, u, cc, xc, cc - gc, v + 0);
+            kkt_col(l, u, cc, xa, cc - ga, v + 5);
+            const double w = __ldg(P.dc2 + j), xl = (double)ld_it<GK>(P.it.x_last + j);
+            v[10] += (xc - xl) * (xc - xl) / w;
+            v[11] += (xa - xl) * (xa - xl) / w;
+        }
+    }
+}
+
+// After a check: copy the new best point, apply a restart (pdlp_algo.hpp:160-174)
+// and, on restart, redo the next primal step with the new primal weight.
+template <int GK, class T>
+__device__ void pass_after_check(const KParams<T>& P, const Ctl& c, const Group& g, int best_sel, int restart,
+                                 int use_avg, double wsum_old, double& dx2) {
+    const bool has_avg = wsum_old > 0;
+    T* x = P.it.x[c.xi];
+    T* xn = P.it.x[1 - c.xi];
+    const double tau = c.eta / c.omega;
+    for (int j = g.gt; j < P.n; j += g.nt) {
+        const T xct = ld_it<GK>(x + j);
+        const double xc = (double)xct;
+        const double xa = has_avg ? __ldcg(P.xsum + j) / wsum_old : xc;
+        if (best_sel == SEL_CUR) P.best_x[j] = xc;
+        else if (best_sel == SEL_AVG) P.best_x[j] = xa;
+        if (restart) {
+            const double cand = use_avg ? xa : xc;
+            P.it.x_last[j] = (T)cand;
+            T xnew = xct;
+            if (use_avg) { xnew = (T)xa; x[j] = xnew; }
+            P.xsum[j] = 0.0;
+            const double gg = (double)ld_it<GK>((use_avg ? P.it.aty[c.aty_avg] : P.it.aty[c.aty_cur]) + j);
+            primal_col<T>(P, j, xnew, gg, tau, xn, dx2);
+        }
+    }
+    T* y = P.it.y[c.yi];
+    for (int i = g.gt; i < P.m; i += g.nt) {
+        const T yct = ld_it<GK>(y + i);
+        const double yc = (double)yct;
+        const double ya = has_avg ? __ldcg(P.ysum + i) / wsum_old : yc;
+        if (best_sel == SEL_CUR) P.best_y[i] = yc;
+        else if (best_sel == SEL_AVG) P.best_y[i] = ya;
+        if (restart) {
+            const double cand = use_avg ? ya : yc;
+            P.it.y_last[i] = (T)cand;
+            if (use_avg) y[i] = (T)ya;
+            P.ysum[i] = 0.0;
+        }
+    }
+}
+
+__device__ __forceinline__ double merit3(double a, double b, double c) { return sqrt(a * a + b * b + c * c); }
+
+// Check decision (pdlp_algo.hpp:135-174) from the 22 check totals; run by one
+// thread per CTA on identical inputs. Returns, through `flags`, which point
+// becomes the best point, whether to restart and whether to the average.
+template <bool FP32>
+__device__ void check_decision(const KParamsBase& B, Ctl& s, const double* t, bool evaluate_only, bool write_trace,
+                               int* flags, double* wsum_old) {
+    double eP[2], eD[2], eG[2], mer[2];
+    for (int o = 0; o < 2; ++o) {
+        const double* r = t + 4 * o;        // rows: rv2, sv2, D, ninf
+        const double* q = t + 10 + 5 * o;   // cols: bv2, sv2, D, ninf, cx
+        eP[o] = sqrt(r[0] + q[0]) / B.denom_p;
+        eD[o] = sqrt(r[1] + q[1]) / B.denom_d;
+        double D = r[2] + q[2];
+        if (r[3] + q[3] > 0) D = -kInfD;
+        const double cx = q[4];
+        eG[o] = isfinite(D) ? fabs(cx - D) / (1.0 + fabs(cx) + fabs(D)) : kInfD;
+        mer[o] = merit3(eP[o], eD[o], eG[o]);
+    }
+    s.checks++;
+    int best_sel = 0, restart = 0, use_avg = 0;
+    *wsum_old = s.wsum;
+    if (evaluate_only) {
+        // stopped before any check: report the current point (pdlp_algo.hpp:178-182)
+        s.out_sel = SEL_CUR;
+        s.out_eps[0] = eP[0]; s.out_eps[1] = eD[0]; s.out_eps[2] = eG[0];
+        flags[0] = flags[1] = flags[2] = 0;
+        return;
+    }
+    if (mer[0] < s.best_merit) {
+        s.best_merit = mer[0]; best_sel = SEL_CUR;
+        s.best_eps[0] = eP[0]; s.best_eps[1] = eD[0]; s.best_eps[2] = eG[0];
+    }
+    if (mer[1] < s.best_merit) {
+        s.best_merit = mer[1]; best_sel = SEL_AVG;
+        s.best_eps[0] = eP[1]; s.best_eps[1] = eD[1]; s.best_eps[2] = eG[1];
+    }
+    if (best_sel) { s.best_valid = 1; s.stall = 0; } else { s.stall++; }
+    use_avg = mer[1] < mer[0];
+    const int o = use_avg ? 1 : 0;
+    const double mc = mer[o];
+    const double worst = fmax(eP[o], fmax(eD[o], eG[o]));
+    if (worst <= B.tol) {
+        if (FP32) {
+            s.switch_req = 1;  // confirm with FP64 iterates before terminating
+            s.check_now = 1;
+        } else {
+            s.exit_reason = B2_EXIT_CONVERGED;
+            s.out_sel = use_avg ? SEL_AVG : SEL_CUR;
+            s.out_eps[0] = eP[o]; s.out_eps[1] = eD[o]; s.out_eps[2] = eG[o];
+        }
+    } else {
+        const bool sufficient = mc <= 0.2 * s.merit_last_restart;
+        const bool necessary = mc <= 0.8 * s.merit_last_restart && mc > s.merit_prev_cand;
+        const bool artificial = s.since_restart >= 0.36 * s.accepted;
+        s.merit_prev_cand = mc;
+        if (sufficient || necessary || artificial) {
+            restart = 1;
+            const double ddx = sqrt(t[20 + o]), ddy = sqrt(t[8 + o]);
+            if (ddx > 1e-10 && ddy > 1e-10) s.omega = exp(0.5 * log(ddy / ddx) + 0.5 * log(s.omega));
+            s.since_restart = 0;
+            s.restarts++;
+            s.merit_last_restart = mc;
+            s.merit_prev_cand = kInfD;
+            s.wsum = 0.0;
+        }
+        if (FP32 && B.mixed && (worst <= B.switch_tol || s.stall >= B.stall_checks)) s.switch_req = 1;
+        if (s.attempts >= B.max_iterations) s.exit_reason = B2_EXIT_MAX_ITER;
+        else if (s.stop_req) s.exit_reason = s.stop_req;
+    }
+    flags[0] = best_sel;
+    flags[1] = restart;
+    flags[2] = use_avg;
+    if (write_trace && B.trace && s.checks - 1 < B.trace_cap) {
+        double* t_out = B.trace + (size_t)(s.checks - 1) * kTraceFields;
+        t_out[0] = s.attempts; t_out[1] = s.accepted;
+        t_out[2] = eP[0]; t_out[3] = eD[0]; t_out[4] = eG[0];
+        t_out[5] = eP[1]; t_out[6] = eD[1]; t_out[7] = eG[1];
+        t_out[8] = s.omega; t_out[9] = s.eta;
+        t_out[10] = restart | (use_avg << 1) | ((FP32 ? 1 : 0) << 2) | (best_sel << 3);
+        t_out[11] = *wsum_old;
+    }
+}
+
+// The KKT check of the current and average points: two passes and two group
+// barriers, then the decision in every CTA. Returns false if a barrier failed.
+template <int GK, class T, class V>
+__device__ bool run_check(const KParams<T>& P, Ctl& s, const Group& g, int lane, bool evaluate_only, double* s_red,
+                          double* s_tot, int* s_flag, double* s_wsum_old) {
+    constexpr bool kFP32 = sizeof(T) == 4;
+    {
+        double v[10];
+#pragma unroll
+        for (int k = 0; k < 10; ++k) v[k] = 0.0;
+        pass_rows_check<GK, T, V>(P, s, g, lane, v);
+        cta_partial<10, GK>(v, g, SLOT_CK, s_red);
+    }
+    if (threadIdx.x == 0) s.pend_y = 0.0;
+    if (!group_sync<GK>(g)) return false;
+    {
+        double v[12];
+#pragma unroll
+        for (int k = 0; k < 12; ++k) v[k] = 0.0;
+        pass_cols_check<GK, T, V>(P, s, g, lane, v);
+        cta_partial_at<12, GK>(v, g, SLOT_CK, 10, s_red);
+    }
+    if (!group_sync<GK>(g)) return false;
+    group_totals<22, GK>(g, SLOT_CK, s_tot);
+    if (threadIdx.x == 0) check_decision<kFP32>(P, s, s_tot, evaluate_only, g.rank == 0, s_flag, s_wsum_old);
+    __syncthreads();
+    return true;
+}
+
+// ------------------------------------------------------------ the solve
+//
+// Per attempt:   rows pass -> barrier -> step decision -> cols pass -> barrier
+// Per check:     rows check -> barrier -> cols check -> barrier -> decision
+//                [-> best copy / restart pass -> barrier]
+// The group's CTAs enter with the same P and leave together. The control
+// state is read from P.ctl at entry and written back by the group's first CTA
+// at exit. Returns false when a barrier wait timed out (abort).
+template <int GK, class T, class V>
+__device__ bool solve_body(const KParams<T>& P, const Group& g) {
+    __shared__ Ctl s;
+    __shared__ double s_red[kWarps * kMaxNV];
+    __shared__ double s_tot[kMaxNV];
+    __shared__ int s_flag[4];
+    __shared__ double s_wsum_old;
+    const int tid = threadIdx.x, lane = tid & 31;
+    constexpr bool kFP32 = sizeof(T) == 4;
+
+    if (tid == 0) s = *P.ctl;
+    __syncthreads();
+    const bool first_check = s.check_now != 0;
+    if (g.rank == 0 && tid == 0 && s.mode == MODE_START) g.bcast[2] = (double)gtimer();
+
+    // ---------------------------------------------------------- start-up
+    if (s.mode == MODE_START) {
+        // x = x0, y = 0, A^T y = 0, sums = 0 (pdlp_algo.hpp:68-84)
+        for (int j = g.gt; j < P.n; j += g.nt) {
+            const T x0 = (T)__ldg(P.x0 + j);
+            P.it.x[s.xi][j] = x0;
+            P.it.x_last[j] = x0;
+            P.it.aty[s.aty_cur][j] = T(0);
+            P.xsum[j] = 0.0;
+        }
+        for (int i = g.gt; i < P.m; i += g.nt) {
+            P.it.y[s.yi][i] = T(0);
+            P.it.y_last[i] = T(0);
+            P.ysum[i] = 0.0;
+        }
+    } else {
+        // resume with FP64 iterates after the FP32 phase
+        for (int j = g.gt; j < P.n; j += g.nt) {
+            P.it.x[s.xi][j] = (T)P.itf.x[s.xi][j];
+            P.it.x_last[j] = (T)P.itf.x_last[j];
+        }
+        for (int i = g.gt; i < P.m; i += g.nt) {
+            P.it.y[s.yi][i] = (T)P.itf.y[s.yi][i];
+            P.it.y_last[i] = (T)P.itf.y_last[i];
+        }
+    }
+    if (P.debug_delay_ns && g.rank == 0 && tid == 0) {
+        // test hook (bounded): hold the first CTA back so the others' barrier wait runs out
+        const unsigned long long t0 = gtimer();
+        while (gtimer() - t0 < P.debug_delay_ns) __nanosleep(1000);
+    }
+    if (!group_sync<GK>(g)) return false;
+    {   // A x (and A^T y when resuming) at this precision
+        const V* vb = vals<V>(P.A);
+        T* ax = P.it.ax[s.ax_cur];
+        for (int k = g.gw; k < P.A.n_slices; k += g.nw) {
+            const int4 sl = __ldg(P.A.slice + k);
+            const T acc = slice_dot<GK, T, V, T>(P.A, vb, sl, lane, P.it.x[s.xi]);
+            const int lg = (int)((uint32_t)sl.y >> kLenBits);
+            const int i = sl.x + (lane >> lg);
+            if ((lane & ((1 << lg) - 1)) == 0 && i < P.m) ax[i] = acc;
+        }
+        if (s.mode == MODE_RESUME) {
+            const V* vt = vals<V>(P.AT);
+            T* aty = P.it.aty[s.aty_cur];
+            for (int k = g.gw; k < P.AT.n_slices; k += g.nw) {
+                const int4 sl = __ldg(P.AT.slice + k);
+                const T acc = slice_dot<GK, T, V, T>(P.AT, vt, sl, lane, P.it.y[s.yi]);
+                const int lg = (int)((uint32_t)sl.y >> kLenBits);
+                const int j = sl.x + (lane >> lg);
+                if ((lane & ((1 << lg) - 1)) == 0 && j < P.n) aty[j] = acc;
+            }
+        }
+    }
+    if (!group_sync<GK>(g)) return false;
+    {   // primal step of the first attempt
+        double dx2[1] = {0.0};
+        const double tau = s.eta / s.omega;
+        for (int j = g.gt; j < P.n; j += g.nt)
+            primal_col<T>(P, j, ld_it<GK>(P.it.x[s.xi] + j), (double)ld_it<GK>(P.it.aty[s.aty_cur] + j), tau,
+                          P.it.x[1 - s.xi], dx2[0]);
+        cta_partial<1, GK>(dx2, g, SLOT_X, s_red);
+    }
+    if (!group_sync<GK>(g)) return false;
+
+    // --------------------------------------------------------- main loop
+    bool check_pending = first_check;
+    for (;;) {
+        if (!check_pending) {
+            // ---- rows pass of one attempt ----
+            const bool poll = (s.attempts & 15) == 0;
+            int hstop = 0;
+            if (poll && g.rank == 0 && tid == 0 && P.host_stop) hstop = *P.host_stop;
+            {
+                double v[2] = {0.0, 0.0};
+                pass_rows_step<GK, T, V>(P, s, g, lane, v);
+                cta_partial<2, GK>(v, g, SLOT_A, s_red);
+            }
+            if (poll && g.rank == 0 && tid == 0) {
+                g.bcast[0] = (double)hstop;
+                g.bcast[1] = (P.time_limit_ns > 0 && (double)gtimer() - g.bcast[2] > P.time_limit_ns) ? 1.0 : 0.0;
+            }
+            if (!group_sync<GK>(g)) return false;
+            step_totals<GK>(g, s_tot);
+            if (tid == 0) {
+                // adaptive step size (pdlp_algo.hpp:107-131)
+                s.attempts++;
+                if (kFP32) s.fp32_attempts++;
+                const double dy2 = s_tot[0], inter = s_tot[1], dx2 = s_tot[2];
+                const double num = s.omega * dx2 + dy2 / s.omega;
+                const double eta_bar = fabs(inter) > 0 ? num / (2.0 * fabs(inter)) : kInfD;
+                const double k1 = s.accepted + 2.0;
+                const double grow = (1.0 + pow(k1, -0.6)) * s.eta;
+                const double eta_next = isfinite(eta_bar) ? fmin((1.0 - pow(k1, -0.3)) * eta_bar, grow) : grow;
+                s.pend_y = 0.0;  // applied by the rows pass just finished
+                s.pend_x = 0.0;
+                if (s.eta <= eta_bar) {
+                    s.xi ^= 1;
+                    s.yi ^= 1;
+                    const int t = s.ax_cur; s.ax_cur = s.ax_nxt; s.ax_nxt = t;
+                    s.pend_x = s.eta;  // x-average update, in the cols pass below
+                    s.pend_y = s.eta;  // y-average update, in the next rows pass
+                    s.wsum += s.eta;
+                    s.accepted++;
+                    s.since_restart++;
+                    s.last_accepted = 1;
+                    if (kFP32) s.fp32_accepted++;
+                } else {
+                    s.last_accepted = 0;
+                }
+                s.eta = eta_next;
+                if (poll) {
+                    if (__ldcg(&g.bcast[0]) != 0.0) s.stop_req = B2_EXIT_STOPPED;
+                    else if (__ldcg(&g.bcast[1]) != 0.0) s.stop_req = B2_EXIT_TIME_LIMIT;
+                }
+                s_flag[0] = (s.last_accepted && (s.accepted % P.check_every) == 0) || s.attempts >= P.max_iterations;
+            }
+            __syncthreads();
+            const bool check_due = s_flag[0] != 0;
+            // ---- cols pass: A^T y' (if accepted) + next primal step ----
+            {
+                double dx2[1] = {0.0};
+                pass_cols_step<GK, T, V>(P, s, g, lane, dx2[0]);
+                cta_partial<1, GK>(dx2, g, SLOT_X, s_red);
+            }
+            if (tid == 0) {
+                s.pend_x = 0.0;
+                if (!check_due && s.stop_req) s.exit_reason = s.stop_req;
+            }
+            if (!group_sync<GK>(g)) return false;
+            if (!check_due) {
+                if (s.exit_reason != 0) break;
+                continue;
+            }
+        }
+        check_pending = false;
+
+        // ---- KKT check on the unscaled problem: current vs average ----
+        if (!run_check<GK, T, V>(P, s, g, lane, false, s_red, s_tot, s_flag, &s_wsum_old)) return false;
+        if (s.exit_reason == B2_EXIT_CONVERGED) break;
+        {
+            const int best_sel = s_flag[0], restart = s_flag[1], use_avg = s_flag[2];
+            if (best_sel != 0 || restart) {
+                double dx2[1] = {0.0};
+                pass_after_check<GK, T>(P, s, g, best_sel, restart, use_avg, s_wsum_old, dx2[0]);
+                if (restart) cta_partial<1, GK>(dx2, g, SLOT_X, s_red);
+                __syncthreads();
+                if (tid == 0 && restart && use_avg) {
+                    int t = s.ax_cur; s.ax_cur = s.ax_avg; s.ax_avg = t;
+                    t = s.aty_cur; s.aty_cur = s.aty_avg; s.aty_avg = t;
+                }
+                if (!group_sync<GK>(g)) return false;
+            }
+        }
+        if (s.switch_req || s.exit_reason != 0) break;
+    }
+
+    // ------------------------------------------------------------- exit
+    if (s.switch_req && s.exit_reason == 0) {
+        // hand the state over to the FP64 phase
+        if (g.rank == 0 && tid == 0) *P.ctl = s;
+        __syncthreads();
+        return true;
+    }
+    if (s.exit_reason != B2_EXIT_CONVERGED && !s.best_valid) {
+        // no check has run yet: evaluate the current point to report it
+        if (!run_check<GK, T, V>(P, s, g, lane, true, s_red, s_tot, s_flag, &s_wsum_old)) return false;
+    } else if (s.exit_reason != B2_EXIT_CONVERGED) {
+        if (tid == 0) {
+            s.out_sel = SEL_BEST;
+            s.out_eps[0] = s.best_eps[0]; s.out_eps[1] = s.best_eps[1]; s.out_eps[2] = s.best_eps[2];
+        }
+        __syncthreads();
+    }
+    {
+        const int sel = P.return_current ? (int)SEL_CUR : s.out_sel;
+        const T* x = P.it.x[s.xi];
+        const T* y = P.it.y[s.yi];
+        const double wsum = s.wsum;
+        for (int j = g.gt; j < P.n; j += g.nt) {
+            const double v = sel == SEL_CUR ? (double)ld_it<GK>(x + j)
+                             : sel == SEL_AVG ? __ldcg(P.xsum + j) / wsum : __ldcg(P.best_x + j);
+            P.out_x[P.perm_c[j]] = v;
+        }
+        for (int i = g.gt; i < P.m; i += g.nt) {
+            const double v = sel == SEL_CUR ? (double)ld_it<GK>(y + i)
+                             : sel == SEL_AVG ? __ldcg(P.ysum + i) / wsum : __ldcg(P.best_y + i);
+            P.out_y[P.perm_r[i]] = v;
+        }
+        __syncthreads();
+        if (g.rank == 0 && tid == 0) { s.out_sel = sel; *P.ctl = s; }
+        __syncthreads();
+    }
+    return true;
+}
+
+// Standalone SpMV of a sliced matrix (y = M x), for b2_engine_spmv and the
+// bandwidth benchmark; the same slice_dot the solver uses.
+template <class AccT, class V, class XT>
+__global__ void __launch_bounds__(256) k_spmv(SellDev S, const XT* x, AccT* y) {
+    const int lane = threadIdx.x & 31;
+    const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, nw = (gridDim.x * blockDim.x) >> 5;
+    const V* vb = vals<V>(S);
+    for (int s = gw; s < S.n_slices; s += nw) {
+        const int4 sl = __ldg(S.slice + s);
+        const AccT acc = slice_dot<GK_GRID, AccT, V, XT>(S, vb, sl, lane, x);
+        const int lg = (int)((uint32_t)sl.y >> kLenBits);
+        const int r = sl.x + (lane >> lg);
+        if ((lane & ((1 << lg) - 1)) == 0 && r < S.n_rows) y[r] = acc;
+    }
+}
+
+}  // namespace dev
+
+// ---------------------------------------------------- host-side helpers
+void cuda_ok(cudaError_t e, const char* what);
+
+template <class T>
+T* dalloc(size_t count, size_t& total) {
+    void* p = nullptr;
+    const size_t bytes = (count > 0 ? count : 1) * sizeof(T);
+    cuda_ok(cudaMalloc(&p, bytes), "cudaMalloc");
+    total += bytes;
+    return static_cast<T*>(p);
+}
+
+}  // namespace b2

@@ -86,4 +86,14 @@ void engine_spmv(EngineImpl* e, int which, const double* x, double* y);
 int engine_trace(EngineImpl* e, double* out, int max_records);
 void engine_spmv_bench(EngineImpl* e, int which, int precision, int reps, void* stream, double* avg_ms);
 
+// The batched engine (batch.cu). All functions throw Error.
+struct BatchImpl;
+BatchImpl* batch_create(int n, const b2_lp_view* U, const b2_lp_view* S, const double* const* Dr,
+                        const double* const* Dc, const b2_solve_opts& o);
+void batch_destroy(BatchImpl* b);
+void batch_solve(BatchImpl* b, const b2_solve_opts& o, const volatile int32_t* stop, b2_result* res, double* ms);
+void batch_solution(BatchImpl* b, int i, double* x, double* y);
+void batch_info(BatchImpl* b, b2_batch_info* inf);
+void batch_spmv(BatchImpl* b, int i, int which, const double* x, double* y);
+
 }  // namespace b2
