@@ -117,6 +117,29 @@ int b2_solve_pdhg_gpu_ex(const b2_lp_view* unscaled_form, const b2_lp_view* scal
                          const double* Dc, const b2_solve_opts* opts, const volatile int32_t* stop_flag,
                          double* x_out, double* y_out, b2_result* res);
 
+/* Allocation-free form of b2_solve_pdhg_gpu_ex (no counterpart in the
+ * reference). For callers that must not allocate device memory: code running
+ * while a CUDA stream is captured into a graph (cudaMalloc is not a capturable
+ * stream operation), processes whose GPU memory belongs to a pool they do not
+ * own, and latency-critical paths that must stay out of the driver's
+ * allocator. It runs the one-CTA solve with its whole device working set
+ * (layout, iterates, averages, control state, outputs) in a static device
+ * array of 32 MiB that every GPU using the library holds until exit; LPs
+ * that need more (roughly above 200,000 nonzeros) get B2_ERR_UNSUPPORTED
+ * before any GPU work. It calls no cudaMalloc / cudaFree or other allocating
+ * CUDA routine (host memory is still used to build the layout). The first
+ * call on a device looks up the array's address with that device current:
+ * make that first call before any stream capture starts. All calls in the
+ * process share the array, which keeps the previous call's contents (each
+ * call clears what must start at zero); calls are serialized by a lock and
+ * return after their GPU work ends, since GPU work of two overlapping calls
+ * would race on the array. Inputs, outputs and options mean what they mean
+ * for b2_solve_pdhg_gpu_ex, except that stop_flag, time limit and stream are
+ * not supported (work runs on the legacy default stream). */
+int b2_solve_pdhg_gpu_noalloc(const b2_lp_view* unscaled_form, const b2_lp_view* scaled_form, const double* Dr,
+                              const double* Dc, const b2_solve_opts* opts, double* x_out, double* y_out,
+                              b2_result* res);
+
 /* ---- resident engine: upload once, solve many times ---------------------
  * b2_engine_create does what the reference's GpuBackend constructor does
  * (gpu/pdlp_gpu_solve.cu:198-205): builds the device layout of A and A^T and

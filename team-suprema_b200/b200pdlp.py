@@ -37,7 +37,8 @@ PREC_FP64, PREC_MIXED = 0, 1
 EXIT_CONVERGED, EXIT_MAX_ITER, EXIT_STOPPED, EXIT_TIME_LIMIT = 1, 2, 3, 4
 
 EXPORTED = [
-    "b2_default_opts", "b2_solve_pdhg_gpu", "b2_solve_pdhg_gpu_ex", "b2_engine_create", "b2_engine_solve",
+    "b2_default_opts", "b2_solve_pdhg_gpu", "b2_solve_pdhg_gpu_ex", "b2_solve_pdhg_gpu_noalloc",
+    "b2_engine_create", "b2_engine_solve",
     "b2_engine_destroy", "b2_engine_get_info", "b2_engine_spmv", "b2_engine_spmv_bench", "b2_engine_trace",
     "b2_batch_create", "b2_batch_solve", "b2_batch_get_solution", "b2_batch_get_info", "b2_batch_spmv",
     "b2_batch_destroy",
@@ -111,6 +112,8 @@ def lib():
                                             vp, vp, vp, C.POINTER(_Result)]
             L.b2_solve_pdhg_gpu_ex.argtypes = [C.POINTER(_LPView), C.POINTER(_LPView), vp, vp,
                                                C.POINTER(SolveOpts), vp, vp, vp, C.POINTER(_Result)]
+            L.b2_solve_pdhg_gpu_noalloc.argtypes = [C.POINTER(_LPView), C.POINTER(_LPView), vp, vp,
+                                                    C.POINTER(SolveOpts), vp, vp, C.POINTER(_Result)]
             L.b2_engine_create.argtypes = [C.POINTER(_LPView), C.POINTER(_LPView), vp, vp, C.POINTER(SolveOpts),
                                            C.POINTER(vp)]
             L.b2_engine_solve.argtypes = [vp, C.POINTER(SolveOpts), vp, vp, vp, C.POINTER(_Result)]

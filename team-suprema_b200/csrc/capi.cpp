@@ -98,6 +98,14 @@ int b2_solve_pdhg_gpu(const b2_lp_view* U, const b2_lp_view* S, const double* Dr
     return b2_solve_pdhg_gpu_ex(U, S, Dr, Dc, &o, stop_flag, x_out, y_out, res);
 }
 
+int b2_solve_pdhg_gpu_noalloc(const b2_lp_view* U, const b2_lp_view* S, const double* Dr, const double* Dc,
+                              const b2_solve_opts* opts, double* x_out, double* y_out, b2_result* res) {
+    return b2::guarded([&] {
+        if (!U || !S || !opts) b2::fail(B2_ERR_INVALID, "null argument");
+        b2::solve_noalloc(*U, *S, Dr, Dc, *opts, x_out, y_out, res);
+    });
+}
+
 int b2_engine_create(const b2_lp_view* U, const b2_lp_view* S, const double* Dr, const double* Dc,
                      const b2_solve_opts* opts, b2_engine** out) {
     return b2::guarded([&] {

@@ -86,6 +86,10 @@ void engine_spmv(EngineImpl* e, int which, const double* x, double* y);
 int engine_trace(EngineImpl* e, double* out, int max_records);
 void engine_spmv_bench(EngineImpl* e, int which, int precision, int reps, void* stream, double* avg_ms);
 
+// The allocation-free one-CTA solve (noalloc.cu). Throws Error.
+void solve_noalloc(const b2_lp_view& U, const b2_lp_view& S, const double* Dr, const double* Dc,
+                   const b2_solve_opts& o, double* x_out, double* y_out, b2_result* res);
+
 // The batched engine (batch.cu). All functions throw Error.
 struct BatchImpl;
 BatchImpl* batch_create(int n, const b2_lp_view* U, const b2_lp_view* S, const double* const* Dr,

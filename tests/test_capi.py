@@ -97,3 +97,17 @@ def test_stop_flag_word_layout():
     assert not f.is_set()
     f.set()
     assert C.c_int32.from_address(f.ptr).value == 1
+
+
+def test_noalloc_rejects_lp_above_its_static_limit():
+    """The allocation-free entry point refuses, before any GPU work, an LP whose
+    device working set exceeds its 32 MiB static array."""
+    lp = B.gen_random_lp(60000, 180000, 6, 1, True)
+    U, S, Dr, Dc, _ = B.prepare(lp)
+    o = B.default_opts()
+    r = B._Result()
+    uv, sv = U.view(), S.view()
+    rc = B.lib().b2_solve_pdhg_gpu_noalloc(C.byref(uv), C.byref(sv), Dr.ctypes.data, Dc.ctypes.data, C.byref(o),
+                                            None, None, C.byref(r))
+    assert rc == B.B2_ERR_UNSUPPORTED
+    assert "32 MiB" in B.lib().b2_last_error().decode()
