@@ -36,6 +36,9 @@ WORKLOADS = {
     "small": ("random", dict(m=600, n=1800, k=6, seed=0, fp32=False)),
     "medium": ("random", dict(m=50_000, n=150_000, k=6, seed=3, fp32=True)),
     "batch": ("batch", dict(count=4096, seed=0)),
+    # Poisson arrivals at 2,000 LPs/s: 80% m~U[100,2000], 19% m~U[2000,50000],
+    # 1% m=500,000; n=3m, 6 nnz/col, per-request seeds (a window of `seconds`)
+    "serve": ("serve", dict(rate=2000.0, seconds=0.1, seed=0)),
 }
 
 
@@ -48,6 +51,9 @@ REF_ATTEMPTS = {"large": 143360, "medium": 73024, "small": 13888}
 
 def describe(name):
     kind, p = WORKLOADS[name]
+    if kind == "serve":
+        return (f"served stream: Poisson arrivals at {p['rate']:.0f} LPs/s for {p['seconds']} s; sizes 80% "
+                f"m~U[100,2000], 19% m~U[2000,50000], 1% m=500000; n=3m, 6 nnz/col, FP32 values, seed {p['seed']}")
     if kind == "batch":
         return (f"batch of {p['count']} random equality LPs, m log-uniform [50,5000], n=round(U[2,4] m), "
                 f"U{{4..10}} nnz/col, FP32 values, seed {p['seed']}")
@@ -277,6 +283,88 @@ def batch_bench(args, world, rank, local):
     bt.close()
 
 
+def serve_stream(rate, seconds, seed):
+    """Arrival times and (m, n, k, seed) of the request stream."""
+    rng = np.random.default_rng(seed)
+    t, out = 0.0, []
+    while True:
+        t += rng.exponential(1.0 / rate)
+        if t >= seconds:
+            return out
+        u = rng.random()
+        if u < 0.80:
+            m = int(rng.integers(100, 2001))
+        elif u < 0.99:
+            m = int(rng.integers(2000, 50001))
+        else:
+            m = 500_000
+        out.append((t, m, 3 * m, 6, int(rng.integers(1, 2**62))))
+
+
+def serve_bench(args, world, rank, local):
+    """One step = the whole request stream: submitted at its arrival times to
+    the server (b2_server_*), every result waited for; value = completed / makespan."""
+    import torch
+    import b200pdlp as B
+    torch.cuda.set_device(local)
+    prec = B.PREC_MIXED if args.precision == "mixed" else B.PREC_FP64
+    _, p = WORKLOADS[args.workload]
+    stream = serve_stream(p["rate"], args.serve_seconds or p["seconds"], p["seed"])
+    t0 = time.time()
+    lps = [B.gen_random_lp(m, n, k, sd, True) for (_, m, n, k, sd) in stream]
+    t_gen = time.time() - t0
+    warm = [B.gen_random_lp(m, 3 * m, 6, 1000 + i, True) for i, m in enumerate((300, 900, 1500))]
+    with B.Server(round_ms=args.round_ms, precision=prec, max_iterations=2_000_000, tol=args.tol) as srv:
+        for _ in range(args.warmup):
+            for t in [srv.submit(w) for w in warm]:
+                srv.wait(t)
+        st0 = srv.stats()
+        dist_barrier(world)
+        tickets = []
+        with ClockSampler(local) as clk:
+            start = time.perf_counter()
+            for (ta, *_), lp in zip(stream, lps):
+                d = start + ta - time.perf_counter()
+                if d > 0:
+                    time.sleep(d)
+                tickets.append(srv.submit(lp))
+            out = [srv.wait(t) for t in tickets]
+            wall = time.perf_counter() - start
+        st1 = srv.stats()
+    dist_barrier(world)
+    lat = np.array([(info["done_s"] - info["submit_s"]) * 1e3 for _, info in out])
+    first = min(info["submit_s"] for _, info in out)
+    last = max(info["done_s"] for _, info in out)
+    makespan = dist_max(last - first, world)
+    value = world * len(out) / makespan
+    conv = sum(r.converged for r, _ in out)
+    worst = max(max(r.eps_P, r.eps_D, r.eps_G) for r, _ in out)
+    lanes = [info["lane"] for _, info in out]
+    sizes = np.array([m for (_, m, *_rest) in stream])
+    if rank == 0:
+        q = lambda a, f: float(np.quantile(a, f)) if len(a) else None  # noqa: E731
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": 1, "warmup": args.warmup,
+            "ms_per_step": makespan * 1e3, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32+f64" if prec == B.PREC_MIXED else "f64", "data": "synthetic",
+            "config": {"workload": describe(args.workload), "requests": len(out),
+                       "offered_per_s": len(out) / (args.serve_seconds or p["seconds"]),
+                       "classes": {"m<=2000": int((sizes <= 2000).sum()),
+                                   "2000<m<=50000": int(((sizes > 2000) & (sizes <= 50000)).sum()),
+                                   "m=500000": int((sizes == 500_000).sum())},
+                       "tol": args.tol, "round_ms": args.round_ms, "hbm_budget_gb": 150,
+                       "parallelism": f"replicas x{world}" if world > 1 else "single GPU"},
+            "latency_ms": {"p50": q(lat, 0.5), "p99": q(lat, 0.99), "p999": q(lat, 0.999), "max": float(lat.max()),
+                           "p50_small": q(lat[sizes <= 2000], 0.5), "p99_small": q(lat[sizes <= 2000], 0.99)},
+            "converged": int(conv), "worst_kkt": worst, "whole_gpu_lane": int(sum(lanes)),
+            "server": {"rounds": st1["rounds"] - st0["rounds"], "grid_slices": st1["grid_slices"] - st0["grid_slices"],
+                       "busy_ms": st1["busy_ms"] - st0["busy_ms"], "peak_bytes": st1["peak_bytes"]},
+            "wall_s": wall, "gen_s": t_gen, "clocks": clk.summary(),
+            "gpu_launches": int(st1["rounds"] - st0["rounds"] + st1["grid_slices"] - st0["grid_slices"]),
+        }
+        print(json.dumps(line), flush=True)
+
+
 def profile_mode(args):
     """Short runs for profiler captures: builds the engine for the workload and
     launches only the kernel under study."""
@@ -315,6 +403,8 @@ def main():
     ap.add_argument("--max-attempts", type=int, default=256, help="--mode solve: attempt limit")
     ap.add_argument("--reps", type=int, default=1, help="--mode spmv: timed launches per product")
     ap.add_argument("--batch-block", type=int, default=0, help="batch: threads per CTA (128/256/512, 0 auto)")
+    ap.add_argument("--serve-seconds", type=float, default=0.0, help="serve: arrival window (0: workload default)")
+    ap.add_argument("--round-ms", type=float, default=5.0, help="serve: device time of one batched round")
     ap.add_argument("--batch-cluster-nnz", type=int, default=0,
                     help="batch: stored entries from which an LP is solved by a cluster (0 auto, <0 never)")
     args = ap.parse_args()
@@ -323,6 +413,8 @@ def main():
         return profile_mode(args)
     if WORKLOADS[args.workload][0] == "batch":
         return batch_bench(args, world, rank, local)
+    if WORKLOADS[args.workload][0] == "serve":
+        return serve_bench(args, world, rank, local)
 
     if args.impl == "reference":
         if args.ref_attempts_per_solve <= 0:

@@ -35,6 +35,7 @@ extern "C" {
 #define B2_ERR_NO_DEVICE 5   /* no CUDA device                                           */
 #define B2_ERR_NONFINITE 6   /* NaN / inf where a finite number is required              */
 #define B2_ERR_UNSUPPORTED 7 /* request outside what this build supports                 */
+#define B2_ERR_PENDING 8     /* b2_server_wait: the request has not finished yet          */
 
 /* ---- one LP, as the reference's RangedLP holds it ---------------------
  * rL <= A x <= rU, l <= x <= u, minimise c'x + obj_offset; A in COO
@@ -211,6 +212,67 @@ int b2_batch_get_info(b2_batch* b, b2_batch_info* info);
  * device layout (FP64 accumulation); x, y in that LP's caller order. */
 int b2_batch_spmv(b2_batch* b, int32_t i, int32_t which, const double* x, double* y);
 void b2_batch_destroy(b2_batch* b);
+
+/* ---- served stream: LPs arriving over time, continuous batching ----------
+ * No counterpart in the reference, which solves one LP per call. A server
+ * owns one GPU (the current device at creation) and three kinds of threads:
+ * callers submit LPs and wait for tickets; preparation threads scale each LP
+ * (Ruiz + Pock-Chambolle as src/scaling.cpp:25-84) and lay it out; one loop
+ * thread admits prepared LPs, oldest first, while their device footprint fits
+ * the HBM budget, uploads them while the GPU works, and runs rounds of the
+ * batched kernel over every resident LP. A round lasts about round_ms of
+ * device time; LPs still running then pause at an attempt boundary with
+ * their state left on the device and go on in the next round, which also
+ * takes in whatever arrived meanwhile. Each LP is solved by one CTA exactly
+ * as one b2_batch LP is: its answer is bit-identical whatever else is in
+ * flight. LPs with at least grid_nnz nonzeros are solved one at a time by the
+ * whole GPU (the b2_engine solve), in slices of grid_slice_ms between rounds.
+ * Every answer carries the engine's device-side KKT figures (the restatement
+ * of the reference's verify(), src/verify.cpp:24-103). */
+typedef struct b2_server b2_server;
+
+typedef struct b2_server_opts {
+    double hbm_budget_bytes;  /* device bytes resident LPs may hold; <= 0: 150e9       */
+    double round_ms;          /* device time of one batched round; <= 0: 5 ms           */
+    int32_t max_resident;     /* LPs resident at once (batched lane); <= 0: 65536       */
+    int32_t prep_threads;     /* host preparation threads; <= 0: hardware threads (<=16) */
+    int64_t grid_nnz;         /* nonzeros from which an LP takes the whole-GPU lane; <= 0: 4,000,000 */
+    double grid_slice_ms;     /* device time of one whole-GPU slice; <= 0: 20 ms        */
+    int64_t cluster_nnz;      /* stored entries (A and A^T) from which a batched LP is solved by
+                                 a cluster of 8 CTAs; 0: 300,000; < 0: never             */
+} b2_server_opts;
+
+typedef struct b2_request_info {
+    double submit_s, admit_s, done_s; /* server clock (seconds since creation)             */
+    double prep_ms;                   /* host scaling + layout                               */
+    int32_t rounds;                   /* rounds (or whole-GPU slices) the LP ran in          */
+    int32_t lane;                     /* 0: batched, 1: whole GPU                            */
+    int64_t device_bytes;             /* its footprint as admitted                           */
+} b2_request_info;
+
+typedef struct b2_server_stats {
+    int64_t submitted, completed, failed;
+    int64_t rounds, grid_slices;
+    int32_t resident, queued;
+    int64_t bytes_in_use, peak_bytes;
+    double busy_ms;                   /* device time of rounds and slices                    */
+} b2_server_stats;
+
+/* opts: solve options for every request (tol, precision, max_iterations, ...);
+ * NULL: b2_default_opts. sopts NULL: all defaults. */
+int b2_server_create(const b2_server_opts* sopts, const b2_solve_opts* opts, b2_server** out);
+/* Submits one LP in unscaled PDLP form (as solve_pdhg_gpu's unscaled_form: rows
+ * `=` or `>=`); the server copies it and returns at once with a ticket. */
+int b2_server_submit(b2_server* s, const b2_lp_view* unscaled_form, int64_t* ticket);
+/* Waits up to timeout_s seconds (< 0: no limit) for a ticket. On B2_OK the
+ * result is handed over (x: n, y: m in unscaled PDLP-form space, any may be
+ * NULL) and the ticket is forgotten; B2_ERR_PENDING: not finished yet. A
+ * request that failed returns its error code, once. */
+int b2_server_wait(b2_server* s, int64_t ticket, double timeout_s, double* x, double* y, b2_result* res,
+                   b2_request_info* info);
+int b2_server_stats_get(b2_server* s, b2_server_stats* out);
+/* Stops the server: running LPs are abandoned, unclaimed results dropped. */
+void b2_server_destroy(b2_server* s);
 
 /* ---- host-side preparation (product side, no GPU needed) ---------------- */
 

@@ -32,7 +32,7 @@ LIB_PATH = os.path.join(HERE, "libb200pdlp.so")
 INCLUDE_H = os.path.join(os.path.dirname(HERE), "include", "b200_pdlp.h")
 
 B2_OK, B2_ERR_INVALID, B2_ERR_CUDA, B2_ERR_OOM, B2_ERR_TIMEOUT, B2_ERR_NO_DEVICE, B2_ERR_NONFINITE, \
-    B2_ERR_UNSUPPORTED = range(8)
+    B2_ERR_UNSUPPORTED, B2_ERR_PENDING = range(9)
 PREC_FP64, PREC_MIXED = 0, 1
 EXIT_CONVERGED, EXIT_MAX_ITER, EXIT_STOPPED, EXIT_TIME_LIMIT = 1, 2, 3, 4
 
@@ -42,6 +42,7 @@ EXPORTED = [
     "b2_engine_destroy", "b2_engine_get_info", "b2_engine_spmv", "b2_engine_spmv_bench", "b2_engine_trace",
     "b2_batch_create", "b2_batch_solve", "b2_batch_get_solution", "b2_batch_get_info", "b2_batch_spmv",
     "b2_batch_destroy",
+    "b2_server_create", "b2_server_submit", "b2_server_wait", "b2_server_stats_get", "b2_server_destroy",
     "b2_scale",
     "b2_gen_random_lp", "b2_gen_transport", "b2_last_error", "b2_version",
 ]
@@ -83,6 +84,24 @@ class BatchInfo(C.Structure):
     _fields_ = [("n_lp", C.c_int32), ("sum_m", C.c_int64), ("sum_n", C.c_int64), ("sum_nnz", C.c_int64),
                 ("sum_padded", C.c_int64), ("max_ctas", C.c_int32), ("threads_per_cta", C.c_int32),
                 ("device_bytes", C.c_int64)]
+
+
+class ServerOpts(C.Structure):
+    _fields_ = [("hbm_budget_bytes", C.c_double), ("round_ms", C.c_double), ("max_resident", C.c_int32),
+                ("prep_threads", C.c_int32), ("grid_nnz", C.c_int64), ("grid_slice_ms", C.c_double),
+                ("cluster_nnz", C.c_int64)]
+
+
+class RequestInfo(C.Structure):
+    _fields_ = [("submit_s", C.c_double), ("admit_s", C.c_double), ("done_s", C.c_double),
+                ("prep_ms", C.c_double), ("rounds", C.c_int32), ("lane", C.c_int32), ("device_bytes", C.c_int64)]
+
+
+class ServerStats(C.Structure):
+    _fields_ = [("submitted", C.c_int64), ("completed", C.c_int64), ("failed", C.c_int64),
+                ("rounds", C.c_int64), ("grid_slices", C.c_int64), ("resident", C.c_int32),
+                ("queued", C.c_int32), ("bytes_in_use", C.c_int64), ("peak_bytes", C.c_int64),
+                ("busy_ms", C.c_double)]
 
 
 class EngineInfo(C.Structure):
@@ -131,6 +150,12 @@ def lib():
             L.b2_batch_spmv.argtypes = [vp, i32, i32, vp, vp]
             L.b2_batch_destroy.argtypes = [vp]
             L.b2_batch_destroy.restype = None
+            L.b2_server_create.argtypes = [C.POINTER(ServerOpts), C.POINTER(SolveOpts), C.POINTER(vp)]
+            L.b2_server_submit.argtypes = [vp, C.POINTER(_LPView), C.POINTER(i64)]
+            L.b2_server_wait.argtypes = [vp, i64, f64, vp, vp, C.POINTER(_Result), C.POINTER(RequestInfo)]
+            L.b2_server_stats_get.argtypes = [vp, C.POINTER(ServerStats)]
+            L.b2_server_destroy.argtypes = [vp]
+            L.b2_server_destroy.restype = None
             L.b2_scale.argtypes = [C.POINTER(_LPView), i32] + [vp] * 8
             L.b2_gen_random_lp.argtypes = [i32, i32, i32, C.c_uint64, i32] + [vp] * 8
             L.b2_gen_transport.argtypes = [i32, i32, C.c_uint64] + [vp] * 8
@@ -429,6 +454,69 @@ class Batch:
         i = BatchInfo()
         _check(lib().b2_batch_get_info(self._h, C.byref(i)))
         return {k: getattr(i, k) for k, _ in BatchInfo._fields_}
+
+
+class Server:
+    """The served stream (b2_server_*): submit LPs in unscaled PDLP form as they
+    arrive; the server scales and lays them out on its own threads, admits
+    them under an HBM budget and solves them by continuous batching (rounds
+    of the batched kernel; LPs keep their state on the device between
+    rounds). wait(ticket) returns (PdlpResult, info dict)."""
+
+    def __init__(self, hbm_budget_bytes: float = 0.0, round_ms: float = 0.0, max_resident: int = 0,
+                 prep_threads: int = 0, grid_nnz: int = 0, grid_slice_ms: float = 0.0, cluster_nnz: int = 0,
+                 **opts):
+        so = ServerOpts(float(hbm_budget_bytes), float(round_ms), int(max_resident), int(prep_threads),
+                        int(grid_nnz), float(grid_slice_ms), int(cluster_nnz))
+        o = default_opts(**opts)
+        h = C.c_void_p()
+        _check(lib().b2_server_create(C.byref(so), C.byref(o), C.byref(h)))
+        self._h = h
+        self._dims = {}
+
+    def close(self):
+        if getattr(self, "_h", None) and self._h.value:
+            lib().b2_server_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def submit(self, unscaled_form: RangedLP) -> int:
+        U = RangedLP.like(unscaled_form)
+        t = C.c_int64()
+        _check(lib().b2_server_submit(self._h, C.byref(U.view()), C.byref(t)))
+        self._dims[t.value] = (U.m, U.n)
+        return t.value
+
+    def wait(self, ticket: int, timeout_s: float = -1.0):
+        """(PdlpResult, info) once the ticket is done; None if timeout_s passed first."""
+        m, n = self._dims[ticket]
+        x = np.zeros(max(n, 1))
+        y = np.zeros(max(m, 1))
+        r = _Result()
+        inf = RequestInfo()
+        rc = lib().b2_server_wait(self._h, int(ticket), float(timeout_s), _ptr(x), _ptr(y), C.byref(r), C.byref(inf))
+        if rc == B2_ERR_PENDING:
+            return None
+        del self._dims[ticket]
+        _check(rc)
+        info = {k: getattr(inf, k) for k, _ in RequestInfo._fields_}
+        return _result(r, x[:n], y[:m]), info
+
+    def stats(self) -> dict:
+        st = ServerStats()
+        _check(lib().b2_server_stats_get(self._h, C.byref(st)))
+        return {k: getattr(st, k) for k, _ in ServerStats._fields_}
 
 
 # ------------------------------------------------------------- host-side prep

@@ -22,87 +22,24 @@
 #include <thread>
 #include <vector>
 
-#include "device.cuh"
+#include "batch.h"
 
 namespace b2 {
 namespace dev {
 
-// Offsets of one LP inside the batch pools.
-struct InstDesc {
-    int m, n, a_nslices, at_nslices;
-    long long a_slice, at_slice, a_cv, at_cv, row_off, col_off;
-    double denom_p, denom_d;
-    int exact32, pad;
-};
-
-struct BatchArgs {
-    int n_inst;
-    const int* order;
-    unsigned* next;
-    const InstDesc* inst;
-    const int4* slice;
-    const uint32_t* col;
-    const float* v32;
-    const double* v64;
-    const double *b, *rU, *dr2, *c, *l, *u, *dc2, *x0;
-    const int32_t *perm_r, *perm_c;
-    Bufs<float> itf;
-    Bufs<double> itd;
-    double *xsum, *ysum, *best_x, *best_y, *out_x, *out_y;
-    Ctl* ctl;
-    double* scratch;  // per CTA: NSLOTS * kPartStride partials + 8 broadcast words
-    const volatile int* host_stop;
-    int* abort;
-    unsigned long long *t_start, *t_end;
-    double tol, switch_tol, time_limit_ns;
-    int max_iterations, check_every, stall_checks, mixed;
-    // large LPs, solved by a whole cluster
-    int n_large;
-    const int* order_large;
-    unsigned* next_large;
-    int* cl_slot;        // per cluster: the LP it is on
-    double* cl_scratch;  // per cluster: partial sums + broadcast words
-};
-
-constexpr int kMaxCluster = 8;
-constexpr int kClusterScratch = NSLOTS * kMaxCluster * kPartStride + 8;
-
-template <class T>
-__device__ Bufs<T> offset_bufs(const Bufs<T>& B, long long row_off, long long col_off) {
-    Bufs<T> o;
-    o.x[0] = B.x[0] + col_off; o.x[1] = B.x[1] + col_off;
-    o.y[0] = B.y[0] + row_off; o.y[1] = B.y[1] + row_off;
-    o.ax[0] = B.ax[0] + row_off; o.ax[1] = B.ax[1] + row_off; o.ax[2] = B.ax[2] + row_off;
-    o.aty[0] = B.aty[0] + col_off; o.aty[1] = B.aty[1] + col_off;
-    o.x_last = B.x_last + col_off;
-    o.y_last = B.y_last + row_off;
-    return o;
-}
-
-__device__ void fill_params(KParamsBase& P, const BatchArgs& B, const InstDesc& d, int i) {
+__device__ void fill_params(KParamsBase& P, const BatchArgs& B, const LpDev& d) {
     P.m = d.m;
     P.n = d.n;
-    P.A.n_rows = d.m;
-    P.A.n_slices = d.a_nslices;
-    P.A.slice = B.slice + d.a_slice;
-    P.A.col = B.col + d.a_cv;
-    P.A.v32 = B.v32 + d.a_cv;
-    P.A.v64 = B.v64 ? B.v64 + d.a_cv : nullptr;
-    P.AT.n_rows = d.n;
-    P.AT.n_slices = d.at_nslices;
-    P.AT.slice = B.slice + d.at_slice;
-    P.AT.col = B.col + d.at_cv;
-    P.AT.v32 = B.v32 + d.at_cv;
-    P.AT.v64 = B.v64 ? B.v64 + d.at_cv : nullptr;
-    P.b = B.b + d.row_off; P.rU = B.rU + d.row_off; P.dr2 = B.dr2 + d.row_off;
-    P.c = B.c + d.col_off; P.l = B.l + d.col_off; P.u = B.u + d.col_off; P.dc2 = B.dc2 + d.col_off;
-    P.x0 = B.x0 + d.col_off;
-    P.itf = offset_bufs(B.itf, d.row_off, d.col_off);
-    P.xsum = B.xsum + d.col_off; P.ysum = B.ysum + d.row_off;
-    P.best_x = B.best_x + d.col_off; P.best_y = B.best_y + d.row_off;
-    P.out_x = B.out_x + d.col_off; P.out_y = B.out_y + d.row_off;
-    P.perm_r = B.perm_r + d.row_off; P.perm_c = B.perm_c + d.col_off;
-    P.ctl = B.ctl + i;
+    P.A = d.A;
+    P.AT = d.AT;
+    P.b = d.b; P.rU = d.rU; P.dr2 = d.dr2;
+    P.c = d.c; P.l = d.l; P.u = d.u; P.dc2 = d.dc2; P.x0 = d.x0;
+    P.itf = d.itf;
+    P.xsum = d.xsum; P.ysum = d.ysum;
+    P.best_x = d.best_x; P.best_y = d.best_y;
+    P.out_x = d.out_x; P.out_y = d.out_y;
+    P.perm_r = d.perm_r; P.perm_c = d.perm_c;
+    P.ctl = d.ctl;
     P.host_stop = B.host_stop;
     P.tol = B.tol;
     P.switch_tol = B.switch_tol;
@@ -120,44 +57,48 @@ __device__ void fill_params(KParamsBase& P, const BatchArgs& B, const InstDesc& 
 }
 
 // One LP solved by a group (one CTA or one cluster): parameters into this
-// CTA's shared copy, the FP32 phase and, when it hands over, the FP64 phase.
+// CTA's shared copy, then the phase the LP is in -- FP32 iterates and, when
+// they hand over, FP64 iterates. Returns the LP's exit reason, 0 when it
+// yielded at the group's deadline (its state stays in its buffers).
 template <int GK>
-__device__ void solve_instance(const BatchArgs& B, int i, const Group& g, KParams<float>& Pf,
-                               KParams<double>& Pd) {
+__device__ int solve_instance(const BatchArgs& B, int i, const Group& g, KParams<float>& Pf,
+                              KParams<double>& Pd, int* s_exact) {
     const int tid = threadIdx.x;
-    const InstDesc d = B.inst[i];
     if (tid == 0) {
-        fill_params(Pf, B, d, i);
-        Pf.it = offset_bufs(B.itf, d.row_off, d.col_off);
-        fill_params(Pd, B, d, i);
-        Pd.it = offset_bufs(B.itd, d.row_off, d.col_off);
-        if (g.rank == 0) B.t_start[i] = gtimer();
+        const LpDev& d = B.lps[i];
+        fill_params(Pf, B, d);
+        Pf.it = d.itf;
+        fill_params(Pd, B, d);
+        Pd.it = d.itd;
+        *s_exact = d.exact32;
+        if (g.rank == 0 && d.ctl->mode == MODE_START) B.t_start[i] = gtimer();
     }
     __syncthreads();
-    bool fp64 = !B.mixed;
-    if (B.mixed) {
+    Ctl* c = Pf.ctl;
+    if (!ld_it<GK>(&c->phase64)) {
         solve_body<GK, float, float>(Pf, g);
-        if (g.rank == 0 && tid == 0) {
-            Ctl* c = B.ctl + i;
-            if (c->switch_req && c->exit_reason == 0) {
-                c->mode = MODE_RESUME;
-                c->switch_req = 0;
-                c->best_merit = kInfD;
-                c->best_valid = 0;
-                c->stall = 0;
-            }
+        group_sync<GK>(g);
+        if (g.rank == 0 && tid == 0 && c->switch_req && c->exit_reason == 0) {
+            c->mode = MODE_RESUME;
+            c->switch_req = 0;
+            c->best_merit = kInfD;
+            c->best_valid = 0;
+            c->stall = 0;
+            c->phase64 = 1;
         }
         group_sync<GK>(g);
-        fp64 = ld_it<GK>(&B.ctl[i].mode) == MODE_RESUME;
     }
-    if (fp64) {
-        if (d.exact32) solve_body<GK, double, float>(Pd, g);
+    // a yield or an exit in the FP32 phase leaves phase64 = 0
+    if (ld_it<GK>(&c->phase64) && ld_it<GK>(&c->exit_reason) == 0) {
+        if (*s_exact) solve_body<GK, double, float>(Pd, g);
         else solve_body<GK, double, double>(Pd, g);
     }
-    if (g.rank == 0 && tid == 0) B.t_end[i] = gtimer();
+    group_sync<GK>(g);
+    const int ex = ld_it<GK>(&c->exit_reason);
+    if (g.rank == 0 && tid == 0 && ex != 0) B.t_end[i] = gtimer();
     __syncthreads();
+    return ex;
 }
-
 __device__ __forceinline__ unsigned cluster_rank() {
     unsigned r;
     asm volatile("mov.u32 %0, %%cluster_ctarank;" : "=r"(r));
@@ -169,17 +110,34 @@ __device__ __forceinline__ unsigned cluster_index() {
     return r;
 }
 
+// Round deadline shared by the whole launch: the first CTA to start fixes the
+// base time; every group yields at its first attempt boundary past base +
+// round_ns, and no CTA takes a new LP after it. 0: no deadline.
+__device__ __forceinline__ unsigned long long launch_deadline(const BatchArgs& B) {
+    if (B.round_ns == 0) return 0ull;
+    const unsigned long long now = gtimer();
+    const unsigned long long old = atomicCAS(B.t0, 0ull, now);
+    return (old == 0ull ? now : old) + B.round_ns;
+}
+
 // CL = CTAs per cluster. With CL > 1 the kernel is launched in clusters of CL
 // CTAs: each cluster first solves large LPs together (one at a time, from the
 // large-LP queue); once that queue is empty its CTAs go on alone and take
 // small LPs from the other queue, like every CTA of a CL = 1 launch.
+// qstatus[k] receives the exit reason of the LP at queue position k (small
+// queue first, then the large queue), 0 when it yielded; positions no group
+// reached keep what the host put there.
 template <int CL, int NT>
 __global__ void __launch_bounds__(NT, 1024 / NT) k_pdlp_batch(const BatchArgs B) {
     __shared__ KParams<float> Pf;
     __shared__ KParams<double> Pd;
-    __shared__ int s_inst;
+    __shared__ int s_inst, s_pos, s_exact;
+    __shared__ unsigned long long s_deadline;
     __shared__ double s_part[NSLOTS * kPartStride];
     const int tid = threadIdx.x, warp = tid >> 5;
+    if (tid == 0) s_deadline = launch_deadline(B);
+    __syncthreads();
+    const unsigned long long deadline = s_deadline;
     if (CL > 1) {
         const int rank = (int)cluster_rank();
         const int cid = (int)cluster_index();
@@ -196,15 +154,21 @@ __global__ void __launch_bounds__(NT, 1024 / NT) k_pdlp_batch(const BatchArgs B)
         g.abort = B.abort;
         g.timeout_ns = 0;
         g.spart = nullptr;
+        g.yield_at = deadline;
         for (;;) {
             if (rank == 0 && tid == 0) {
-                const unsigned k = atomicAdd(B.next_large, 1u);
-                B.cl_slot[cid] = k < (unsigned)B.n_large ? B.order_large[k] : -1;
+                int i = -1;
+                if (deadline == 0 || gtimer() < deadline) {
+                    const unsigned k = atomicAdd(B.next_large, 1u);
+                    if (k < (unsigned)B.n_large) { i = B.order_large[k]; s_pos = B.n_inst + (int)k; }
+                }
+                B.cl_slot[cid] = i;
             }
             group_sync<GK_CLUSTER>(g);
             const int i = __ldcg(&B.cl_slot[cid]);
             if (i < 0) break;
-            solve_instance<GK_CLUSTER>(B, i, g, Pf, Pd);
+            const int ex = solve_instance<GK_CLUSTER>(B, i, g, Pf, Pd, &s_exact);
+            if (rank == 0 && tid == 0) B.qstatus[s_pos] = ex;
         }
     }
     Group g;
@@ -220,15 +184,21 @@ __global__ void __launch_bounds__(NT, 1024 / NT) k_pdlp_batch(const BatchArgs B)
     g.abort = B.abort;
     g.timeout_ns = 0;
     g.spart = s_part;
+    g.yield_at = deadline;
     for (;;) {
         if (tid == 0) {
-            const unsigned k = atomicAdd(B.next, 1u);
-            s_inst = k < (unsigned)B.n_inst ? B.order[k] : -1;
+            int i = -1;
+            if (deadline == 0 || gtimer() < deadline) {
+                const unsigned k = atomicAdd(B.next, 1u);
+                if (k < (unsigned)B.n_inst) { i = B.order[k]; s_pos = (int)k; }
+            }
+            s_inst = i;
         }
         __syncthreads();
         const int i = s_inst;
         if (i < 0) break;
-        solve_instance<GK_CTA>(B, i, g, Pf, Pd);
+        const int ex = solve_instance<GK_CTA>(B, i, g, Pf, Pd, &s_exact);
+        if (tid == 0) B.qstatus[s_pos] = ex;
     }
 }
 
@@ -241,7 +211,30 @@ template __global__ void k_pdlp_batch<kMaxCluster, 512>(const BatchArgs B);
 
 }  // namespace dev
 
+// ---- host-side launch helpers (also used by serve.cu) ----
 namespace {
+
+using BatchKernel = void (*)(dev::BatchArgs);
+
+BatchKernel batch_kernel(int cl, int nt) {
+    if (cl == 1) return nt == 128 ? dev::k_pdlp_batch<1, 128> : nt == 256 ? dev::k_pdlp_batch<1, 256>
+                                                                         : dev::k_pdlp_batch<1, 512>;
+    return nt == 128 ? dev::k_pdlp_batch<dev::kMaxCluster, 128>
+                     : nt == 256 ? dev::k_pdlp_batch<dev::kMaxCluster, 256> : dev::k_pdlp_batch<dev::kMaxCluster, 512>;
+}
+
+void cluster_cfg(cudaLaunchConfig_t& cfg, cudaLaunchAttribute* at, int n_clusters, int nt, cudaStream_t st) {
+    cfg.gridDim = dim3(n_clusters * dev::kMaxCluster);
+    cfg.blockDim = dim3(nt);
+    cfg.dynamicSmemBytes = 0;
+    cfg.stream = st;
+    at[0].id = cudaLaunchAttributeClusterDimension;
+    at[0].val.clusterDim.x = dev::kMaxCluster;
+    at[0].val.clusterDim.y = 1;
+    at[0].val.clusterDim.z = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+}
 
 template <class T>
 T* upload_vec(const std::vector<T>& h, size_t& total) {
@@ -252,14 +245,50 @@ T* upload_vec(const std::vector<T>& h, size_t& total) {
 
 }  // namespace
 
+void batch_kernel_shape(int sm_count, BatchShape& out) {
+    for (int v = 0; v < 3; ++v) {
+        const int nt = 128 << v;
+        int occ = 0;
+        cuda_ok(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, batch_kernel(1, nt), nt, 0), "occ");
+        if (occ < 1) fail(B2_ERR_CUDA, "batched kernel does not fit on an SM");
+        out.max_ctas_nt[v] = occ * sm_count;
+        cudaLaunchConfig_t cfg = {};
+        cudaLaunchAttribute at[1];
+        cluster_cfg(cfg, at, 1, nt, nullptr);
+        int ncl = 0;
+        if (cudaOccupancyMaxActiveClusters(&ncl, batch_kernel(dev::kMaxCluster, nt), &cfg) != cudaSuccess) {
+            cudaGetLastError();
+            ncl = 0;
+        }
+        out.max_clusters_nt[v] = ncl;
+    }
+}
+
+void batch_kernel_launch(const dev::BatchArgs& B, bool clusters, int nt, int units, cudaStream_t st) {
+    if (clusters) {
+        cudaLaunchConfig_t cfg = {};
+        cudaLaunchAttribute at[1];
+        cluster_cfg(cfg, at, units, nt, st);
+        cuda_ok(cudaLaunchKernelEx(&cfg, batch_kernel(dev::kMaxCluster, nt), B), "k_pdlp_batch launch");
+    } else {
+        batch_kernel(1, nt)<<<units, nt, 0, st>>>(B);
+        cuda_ok(cudaGetLastError(), "k_pdlp_batch launch");
+    }
+}
+
+// Offsets of one LP inside the batch pools.
+struct PoolOffsets {
+    int64_t a_slice, at_slice, a_cv, at_cv, row_off, col_off;
+};
+
 struct BatchImpl {
     int n = 0, sm_count = 0, max_ctas = 0, last_nt = 256;
-    int max_ctas_nt[3] = {0, 0, 0}, max_clusters_nt[3] = {0, 0, 0};
+    BatchShape shape{};
     cudaStream_t stream = nullptr;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     std::vector<Layout> L;
-    std::vector<dev::InstDesc> desc;
-    std::vector<int64_t> row_off, col_off;
+    std::vector<PoolOffsets> off;
+    std::vector<dev::LpDev> lps;  // host copy of the descriptors
     std::vector<int> order;
     int64_t sum_m = 0, sum_n = 0, sum_nnz = 0, sum_padded = 0;
     size_t bytes = 0;
@@ -298,6 +327,18 @@ struct BatchImpl {
         for (auto& p : B.aty) p = alloc<T>(sum_n);
         B.x_last = alloc<T>(sum_n);
         B.y_last = alloc<T>(sum_m);
+    }
+
+    template <class T>
+    static dev::Bufs<T> offset_bufs(const dev::Bufs<T>& B, int64_t row_off, int64_t col_off) {
+        dev::Bufs<T> o;
+        o.x[0] = B.x[0] + col_off; o.x[1] = B.x[1] + col_off;
+        o.y[0] = B.y[0] + row_off; o.y[1] = B.y[1] + row_off;
+        o.ax[0] = B.ax[0] + row_off; o.ax[1] = B.ax[1] + row_off; o.ax[2] = B.ax[2] + row_off;
+        o.aty[0] = B.aty[0] + col_off; o.aty[1] = B.aty[1] + col_off;
+        o.x_last = B.x_last + col_off;
+        o.y_last = B.y_last + row_off;
+        return o;
     }
 
     void create(int n_lp, const b2_lp_view* U, const b2_lp_view* S, const double* const* Dr, const double* const* Dc,
@@ -340,25 +381,18 @@ struct BatchImpl {
         cuda_ok(cudaEventCreate(&ev1), "event");
 
         // pack
-        desc.resize(n);
-        row_off.resize(n);
-        col_off.resize(n);
+        off.resize(n);
         int64_t slices = 0, cv = 0;
         bool any64 = false;
         for (int i = 0; i < n; ++i) {
             const Layout& l = L[i];
-            dev::InstDesc& d = desc[i];
-            d.m = l.m; d.n = l.n;
-            d.a_nslices = (int)l.A.n_slices(); d.at_nslices = (int)l.AT.n_slices();
+            PoolOffsets& d = off[i];
             d.a_slice = slices; slices += l.A.n_slices();
             d.at_slice = slices; slices += l.AT.n_slices();
             d.a_cv = cv; cv += l.A.padded;
             d.at_cv = cv; cv += l.AT.padded;
-            d.row_off = row_off[i] = sum_m; sum_m += l.m;
-            d.col_off = col_off[i] = sum_n; sum_n += l.n;
-            d.denom_p = l.denom_p; d.denom_d = l.denom_d;
-            d.exact32 = l.exact32 ? 1 : 0;
-            d.pad = 0;
+            d.row_off = sum_m; sum_m += l.m;
+            d.col_off = sum_n; sum_n += l.n;
             any64 |= !l.exact32;
             sum_nnz += l.nnz;
             sum_padded += l.A.padded + l.AT.padded;
@@ -371,7 +405,7 @@ struct BatchImpl {
         std::vector<int32_t> hpr(sum_m), hpc(sum_n);
         for (int i = 0; i < n; ++i) {
             const Layout& l = L[i];
-            const dev::InstDesc& d = desc[i];
+            const PoolOffsets& d = off[i];
             std::copy(l.A.slice.begin(), l.A.slice.end(), h_slice.begin() + d.a_slice * 4);
             std::copy(l.AT.slice.begin(), l.AT.slice.end(), h_slice.begin() + d.at_slice * 4);
             std::copy(l.A.col.begin(), l.A.col.end(), h_col.begin() + d.a_cv);
@@ -401,47 +435,61 @@ struct BatchImpl {
         });
 
         dev::BatchArgs& B = args;
-        B.n_inst = n;
         B.order = alloc<int>(n);
         B.next = alloc<unsigned>(1);
         B.order_large = alloc<int>(n);
         B.next_large = alloc<unsigned>(1);
-        B.inst = up(desc);
-        B.slice = reinterpret_cast<const int4*>(up(h_slice));
-        B.col = up(h_col);
-        B.v32 = up(h_v32);
-        B.v64 = any64 ? up(h_v64) : nullptr;
-        B.b = up(hb); B.rU = up(hrU); B.dr2 = up(hdr2);
-        B.c = up(hc); B.l = up(hl); B.u = up(hu); B.dc2 = up(hdc2); B.x0 = up(hx0);
-        B.perm_r = up(hpr); B.perm_c = up(hpc);
-        alloc_bufs(B.itf);
-        alloc_bufs(B.itd);
-        B.xsum = alloc<double>(sum_n); B.ysum = alloc<double>(sum_m);
-        B.best_x = alloc<double>(sum_n); B.best_y = alloc<double>(sum_m);
-        B.out_x = alloc<double>(sum_n); B.out_y = alloc<double>(sum_m);
-        B.ctl = alloc<dev::Ctl>(n);
+        const int4* slice = reinterpret_cast<const int4*>(up(h_slice));
+        const uint32_t* col = up(h_col);
+        const float* v32 = up(h_v32);
+        const double* v64 = any64 ? up(h_v64) : nullptr;
+        const double *b = up(hb), *rU = up(hrU), *dr2 = up(hdr2);
+        const double *c = up(hc), *l = up(hl), *u = up(hu), *dc2 = up(hdc2), *x0 = up(hx0);
+        const int32_t *perm_r = up(hpr), *perm_c = up(hpc);
+        dev::Bufs<float> itf{};
+        dev::Bufs<double> itd{};
+        alloc_bufs(itf);
+        alloc_bufs(itd);
+        double* xsum = alloc<double>(sum_n); double* ysum = alloc<double>(sum_m);
+        double* best_x = alloc<double>(sum_n); double* best_y = alloc<double>(sum_m);
+        double* out_x = alloc<double>(sum_n); double* out_y = alloc<double>(sum_m);
+        dev::Ctl* ctl = alloc<dev::Ctl>(n);
+        lps.resize(n);
+        for (int i = 0; i < n; ++i) {
+            const Layout& li = L[i];
+            const PoolOffsets& d = off[i];
+            dev::LpDev& q = lps[i];
+            std::memset(&q, 0, sizeof(q));
+            q.m = li.m; q.n = li.n;
+            q.A.n_rows = li.m; q.A.n_slices = (int)li.A.n_slices();
+            q.A.slice = slice + d.a_slice; q.A.col = col + d.a_cv; q.A.v32 = v32 + d.a_cv;
+            q.A.v64 = v64 ? v64 + d.a_cv : nullptr;
+            q.AT.n_rows = li.n; q.AT.n_slices = (int)li.AT.n_slices();
+            q.AT.slice = slice + d.at_slice; q.AT.col = col + d.at_cv; q.AT.v32 = v32 + d.at_cv;
+            q.AT.v64 = v64 ? v64 + d.at_cv : nullptr;
+            q.b = b + d.row_off; q.rU = rU + d.row_off; q.dr2 = dr2 + d.row_off;
+            q.c = c + d.col_off; q.l = l + d.col_off; q.u = u + d.col_off; q.dc2 = dc2 + d.col_off;
+            q.x0 = x0 + d.col_off;
+            q.perm_r = perm_r + d.row_off; q.perm_c = perm_c + d.col_off;
+            q.itf = offset_bufs(itf, d.row_off, d.col_off);
+            q.itd = offset_bufs(itd, d.row_off, d.col_off);
+            q.xsum = xsum + d.col_off; q.ysum = ysum + d.row_off;
+            q.best_x = best_x + d.col_off; q.best_y = best_y + d.row_off;
+            q.out_x = out_x + d.col_off; q.out_y = out_y + d.row_off;
+            q.ctl = ctl + i;
+            q.denom_p = li.denom_p; q.denom_d = li.denom_d;
+            q.exact32 = li.exact32 ? 1 : 0;
+        }
+        B.lps = up(lps);
         B.abort = alloc<int>(1);
         B.t_start = alloc<unsigned long long>(n);
         B.t_end = alloc<unsigned long long>(n);
-        for (int v = 0; v < 3; ++v) {
-            const int nt = 128 << v;
-            int occ = 0;
-            cuda_ok(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kernel(1, nt), nt, 0), "occ");
-            if (occ < 1) fail(B2_ERR_CUDA, "batched kernel does not fit on an SM");
-            max_ctas_nt[v] = occ * sm_count;
-            // clusters of kMaxCluster CTAs for the large LPs
-            cudaLaunchConfig_t cfg = {};
-            cudaLaunchAttribute at[1];
-            cluster_cfg(cfg, at, 1, nt);
-            int ncl = 0;
-            if (cudaOccupancyMaxActiveClusters(&ncl, kernel(dev::kMaxCluster, nt), &cfg) != cudaSuccess) {
-                cudaGetLastError();
-                ncl = 0;
-            }
-            max_clusters_nt[v] = ncl;
-        }
-        max_ctas = *std::max_element(max_ctas_nt, max_ctas_nt + 3);
-        const int ncl_max = *std::max_element(max_clusters_nt, max_clusters_nt + 3);
+        B.t0 = alloc<unsigned long long>(1);
+        B.qstatus = alloc<int>(n);
+        B.round_ns = 0;
+        batch_kernel_shape(sm_count, shape);
+        max_ctas = *std::max_element(shape.max_ctas_nt, shape.max_ctas_nt + 3);
+        const int ncl_max = *std::max_element(shape.max_clusters_nt, shape.max_clusters_nt + 3);
         B.scratch = alloc<double>((size_t)max_ctas * 8);
         B.cl_slot = alloc<int>(std::max(1, ncl_max));
         B.cl_scratch = alloc<double>((size_t)std::max(1, ncl_max) * dev::kClusterScratch);
@@ -451,36 +499,14 @@ struct BatchImpl {
         B.host_stop = d_stop;
         cuda_ok(cudaDeviceSynchronize(), "batch create");
         // host copies of the big layout arrays are no longer needed
-        for (auto& l : L) {
-            std::vector<uint32_t>().swap(l.A.col);
-            std::vector<uint32_t>().swap(l.AT.col);
-            std::vector<float>().swap(l.A.val32);
-            std::vector<float>().swap(l.AT.val32);
-            std::vector<double>().swap(l.A.val64);
-            std::vector<double>().swap(l.AT.val64);
+        for (auto& li : L) {
+            std::vector<uint32_t>().swap(li.A.col);
+            std::vector<uint32_t>().swap(li.AT.col);
+            std::vector<float>().swap(li.A.val32);
+            std::vector<float>().swap(li.AT.val32);
+            std::vector<double>().swap(li.A.val64);
+            std::vector<double>().swap(li.AT.val64);
         }
-    }
-
-    static void (*kernel(int cl, int nt))(dev::BatchArgs) {
-        if (cl == 1) return nt == 128 ? dev::k_pdlp_batch<1, 128> : nt == 256 ? dev::k_pdlp_batch<1, 256>
-                                                                             : dev::k_pdlp_batch<1, 512>;
-        return nt == 128 ? dev::k_pdlp_batch<dev::kMaxCluster, 128>
-                         : nt == 256 ? dev::k_pdlp_batch<dev::kMaxCluster, 256> : dev::k_pdlp_batch<dev::kMaxCluster, 512>;
-    }
-
-    static int nt_index(int nt) { return nt == 128 ? 0 : nt == 256 ? 1 : 2; }
-
-    void cluster_cfg(cudaLaunchConfig_t& cfg, cudaLaunchAttribute* at, int n_clusters, int nt) {
-        cfg.gridDim = dim3(n_clusters * dev::kMaxCluster);
-        cfg.blockDim = dim3(nt);
-        cfg.dynamicSmemBytes = 0;
-        cfg.stream = stream;
-        at[0].id = cudaLaunchAttributeClusterDimension;
-        at[0].val.clusterDim.x = dev::kMaxCluster;
-        at[0].val.clusterDim.y = 1;
-        at[0].val.clusterDim.z = 1;
-        cfg.attrs = at;
-        cfg.numAttrs = 1;
     }
 
     void solve(const b2_solve_opts& o, const volatile int32_t* stop_flag, b2_result* res, double* total_ms) {
@@ -492,24 +518,16 @@ struct BatchImpl {
         // CTA-time than they save)
         const int64_t big = o.batch_cluster_nnz > 0 ? o.batch_cluster_nnz : INT64_MAX;
         const int nt = o.batch_block == 128 || o.batch_block == 256 ? o.batch_block : 512;
-        const int ntx = nt_index(nt);
+        const int ntx = batch_nt_index(nt);
         last_nt = nt;
         std::vector<int> small_q, large_q;
         for (int i : order) {
-            if (max_clusters_nt[ntx] > 0 && L[i].A.padded + L[i].AT.padded >= big) large_q.push_back(i);
+            if (shape.max_clusters_nt[ntx] > 0 && L[i].A.padded + L[i].AT.padded >= big) large_q.push_back(i);
             else small_q.push_back(i);
         }
         if (o.max_iterations < 0) fail(B2_ERR_INVALID, "max_iterations < 0");
         std::vector<dev::Ctl> h(n);
-        for (int i = 0; i < n; ++i) {
-            dev::Ctl& c = h[i];
-            std::memset(&c, 0, sizeof(c));
-            c.eta = L[i].eta0;
-            c.omega = L[i].omega0;
-            c.merit_last_restart = c.merit_prev_cand = c.best_merit = std::numeric_limits<double>::infinity();
-            c.ax_cur = 0; c.ax_nxt = 1; c.ax_avg = 2; c.aty_cur = 0; c.aty_avg = 1;
-            c.mode = dev::MODE_START;
-        }
+        for (int i = 0; i < n; ++i) init_ctl(h[i], L[i], o.precision != B2_PREC_MIXED);
         dev::BatchArgs B = args;
         B.n_inst = (int)small_q.size();
         B.n_large = (int)large_q.size();
@@ -524,25 +542,22 @@ struct BatchImpl {
         B.check_every = std::max(1, o.check_every);
         B.stall_checks = o.stall_checks > 0 ? o.stall_checks : 32;
         B.mixed = o.precision == B2_PREC_MIXED;
+        B.round_ns = 0;
         *h_stop = stop_flag ? *stop_flag : 0;
-        cuda_ok(cudaMemcpyAsync(B.ctl, h.data(), sizeof(dev::Ctl) * n, cudaMemcpyHostToDevice, st), "ctl upload");
+        cuda_ok(cudaMemcpyAsync(lps_ctl(0), h.data(), sizeof(dev::Ctl) * n, cudaMemcpyHostToDevice, st), "ctl upload");
         cuda_ok(cudaMemsetAsync(B.next, 0, sizeof(unsigned), st), "memset");
         cuda_ok(cudaMemsetAsync(B.next_large, 0, sizeof(unsigned), st), "memset");
         cuda_ok(cudaMemsetAsync(B.abort, 0, sizeof(int), st), "memset");
+        cuda_ok(cudaMemsetAsync(B.t0, 0, sizeof(unsigned long long), st), "memset");
         cuda_ok(cudaEventRecord(ev0, st), "event");
         if (!large_q.empty()) {
-            cudaLaunchConfig_t cfg = {};
-            cudaLaunchAttribute at[1];
-            int ncl = max_clusters_nt[ntx];
+            int ncl = shape.max_clusters_nt[ntx];
             if (o.max_ctas > 0) ncl = std::max(1, std::min(ncl, o.max_ctas / dev::kMaxCluster));
-            cluster_cfg(cfg, at, ncl, nt);
-            cfg.stream = st;
-            cuda_ok(cudaLaunchKernelEx(&cfg, kernel(dev::kMaxCluster, nt), (const dev::BatchArgs)B), "k_pdlp_batch launch");
+            batch_kernel_launch(B, true, nt, ncl, st);
         } else {
-            const int ctas = std::max(1, std::min(max_ctas_nt[ntx], o.max_ctas > 0 ? std::min(o.max_ctas, n) : n));
-            kernel(1, nt)<<<ctas, nt, 0, st>>>(B);
+            const int ctas = std::max(1, std::min(shape.max_ctas_nt[ntx], o.max_ctas > 0 ? std::min(o.max_ctas, n) : n));
+            batch_kernel_launch(B, false, nt, ctas, st);
         }
-        cuda_ok(cudaGetLastError(), "k_pdlp_batch launch");
         cuda_ok(cudaEventRecord(ev1, st), "event");
         for (;;) {
             cudaError_t q = cudaEventQuery(ev1);
@@ -555,40 +570,28 @@ struct BatchImpl {
         cuda_ok(cudaEventElapsedTime(&ms, ev0, ev1), "elapsed");
         if (total_ms) *total_ms = ms;
         last_ctl.resize(n);
-        cuda_ok(cudaMemcpy(last_ctl.data(), B.ctl, sizeof(dev::Ctl) * n, cudaMemcpyDeviceToHost), "ctl download");
+        cuda_ok(cudaMemcpy(last_ctl.data(), lps_ctl(0), sizeof(dev::Ctl) * n, cudaMemcpyDeviceToHost), "ctl download");
         std::vector<unsigned long long> t0(n), t1(n);
         cuda_ok(cudaMemcpy(t0.data(), B.t_start, sizeof(unsigned long long) * n, cudaMemcpyDeviceToHost), "t0");
         cuda_ok(cudaMemcpy(t1.data(), B.t_end, sizeof(unsigned long long) * n, cudaMemcpyDeviceToHost), "t1");
         if (res) {
             for (int i = 0; i < n; ++i) {
-                const dev::Ctl& f = last_ctl[i];
-                b2_result& r = res[i];
-                std::memset(&r, 0, sizeof(r));
-                r.iterations = f.attempts;
-                r.restarts = f.restarts;
-                r.converged = f.exit_reason == B2_EXIT_CONVERGED;
-                r.accepted = f.accepted;
-                r.eps_P = f.out_eps[0];
-                r.eps_D = f.out_eps[1];
-                r.eps_G = f.out_eps[2];
-                r.exit_reason = f.exit_reason;
-                r.checks = f.checks;
-                r.fp32_attempts = f.fp32_attempts;
-                r.fp32_accepted = f.fp32_accepted;
-                r.device_ms = (double)(t1[i] - t0[i]) * 1e-6;
-                r.final_eta = f.eta;
-                r.final_omega = f.omega;
-                r.objective = std::numeric_limits<double>::quiet_NaN();
+                fill_result(last_ctl[i], res[i]);
+                res[i].device_ms = (double)(t1[i] - t0[i]) * 1e-6;
+                res[i].objective = std::numeric_limits<double>::quiet_NaN();
             }
         }
     }
 
+    // control states of the batch are contiguous (one pool)
+    dev::Ctl* lps_ctl(int i) const { return lps[0].ctl + i; }
+
     void solution(int i, double* x, double* y) {
         if (i < 0 || i >= n) fail(B2_ERR_INVALID, "LP index out of range");
         if (x && L[i].n)
-            cuda_ok(cudaMemcpy(x, args.out_x + col_off[i], sizeof(double) * L[i].n, cudaMemcpyDeviceToHost), "x");
+            cuda_ok(cudaMemcpy(x, lps[i].out_x, sizeof(double) * L[i].n, cudaMemcpyDeviceToHost), "x");
         if (y && L[i].m)
-            cuda_ok(cudaMemcpy(y, args.out_y + row_off[i], sizeof(double) * L[i].m, cudaMemcpyDeviceToHost), "y");
+            cuda_ok(cudaMemcpy(y, lps[i].out_y, sizeof(double) * L[i].m, cudaMemcpyDeviceToHost), "y");
     }
 
     // y = A x (which 0) or A^T x (which 1) of LP i through the packed pools
@@ -596,33 +599,7 @@ struct BatchImpl {
     void spmv(int i, int which, const double* x, double* y) {
         if (i < 0 || i >= n) fail(B2_ERR_INVALID, "LP index out of range");
         const Layout& l = L[i];
-        const dev::InstDesc& d = desc[i];
-        dev::SellDev S{};
-        S.n_rows = which == 0 ? d.m : d.n;
-        S.n_slices = which == 0 ? d.a_nslices : d.at_nslices;
-        S.slice = args.slice + (which == 0 ? d.a_slice : d.at_slice);
-        S.col = args.col + (which == 0 ? d.a_cv : d.at_cv);
-        S.v32 = args.v32 + (which == 0 ? d.a_cv : d.at_cv);
-        S.v64 = args.v64 ? args.v64 + (which == 0 ? d.a_cv : d.at_cv) : nullptr;
-        const int rows = which == 0 ? l.m : l.n, cols = which == 0 ? l.n : l.m;
-        const std::vector<int32_t>& in_perm = which == 0 ? l.perm_c : l.perm_r;
-        const std::vector<int32_t>& out_perm = which == 0 ? l.perm_r : l.perm_c;
-        std::vector<double> xd(std::max(cols, 1)), yd(std::max(rows, 1));
-        for (int j = 0; j < cols; ++j) xd[j] = x[in_perm[j]];
-        double *dx = nullptr, *dy = nullptr;
-        cuda_ok(cudaMalloc(&dx, xd.size() * sizeof(double)), "cudaMalloc");
-        cuda_ok(cudaMalloc(&dy, yd.size() * sizeof(double)), "cudaMalloc");
-        cuda_ok(cudaMemcpy(dx, xd.data(), xd.size() * sizeof(double), cudaMemcpyHostToDevice), "H2D");
-        if (S.n_slices > 0) {
-            if (l.exact32) dev::k_spmv<double, float, double><<<std::max(1, S.n_slices / 8 + 1), 256, 0, stream>>>(S, dx, dy);
-            else dev::k_spmv<double, double, double><<<std::max(1, S.n_slices / 8 + 1), 256, 0, stream>>>(S, dx, dy);
-        }
-        cuda_ok(cudaGetLastError(), "k_spmv");
-        cuda_ok(cudaStreamSynchronize(stream), "k_spmv");
-        cuda_ok(cudaMemcpy(yd.data(), dy, yd.size() * sizeof(double), cudaMemcpyDeviceToHost), "D2H");
-        cudaFree(dx);
-        cudaFree(dy);
-        for (int r = 0; r < rows; ++r) y[out_perm[r]] = yd[r];
+        spmv_sell(which == 0 ? lps[i].A : lps[i].AT, l, which, l.exact32, stream, x, y);
     }
 
     void info(b2_batch_info* inf) {
@@ -637,6 +614,59 @@ struct BatchImpl {
         inf->device_bytes = (int64_t)bytes;
     }
 };
+
+// Initial control state of an LP (pdlp_algo.hpp:67-102).
+void init_ctl(dev::Ctl& c, const Layout& l, bool fp64_only) {
+    std::memset(&c, 0, sizeof(c));
+    c.eta = l.eta0;
+    c.omega = l.omega0;
+    c.merit_last_restart = c.merit_prev_cand = c.best_merit = std::numeric_limits<double>::infinity();
+    c.ax_cur = 0; c.ax_nxt = 1; c.ax_avg = 2; c.aty_cur = 0; c.aty_avg = 1;
+    c.mode = dev::MODE_START;
+    c.phase64 = fp64_only ? 1 : 0;
+}
+
+void fill_result(const dev::Ctl& f, b2_result& r) {
+    std::memset(&r, 0, sizeof(r));
+    r.iterations = f.attempts;
+    r.restarts = f.restarts;
+    r.converged = f.exit_reason == B2_EXIT_CONVERGED;
+    r.accepted = f.accepted;
+    r.eps_P = f.out_eps[0];
+    r.eps_D = f.out_eps[1];
+    r.eps_G = f.out_eps[2];
+    r.exit_reason = f.exit_reason;
+    r.checks = f.checks;
+    r.fp32_attempts = f.fp32_attempts;
+    r.fp32_accepted = f.fp32_accepted;
+    r.final_eta = f.eta;
+    r.final_omega = f.omega;
+}
+
+// y = M x through a device sliced matrix (FP64 accumulation); x, y in the
+// caller's order of that LP.
+void spmv_sell(const dev::SellDev& S, const Layout& l, int which, bool exact32, cudaStream_t stream, const double* x,
+               double* y) {
+    const int rows = which == 0 ? l.m : l.n, cols = which == 0 ? l.n : l.m;
+    const std::vector<int32_t>& in_perm = which == 0 ? l.perm_c : l.perm_r;
+    const std::vector<int32_t>& out_perm = which == 0 ? l.perm_r : l.perm_c;
+    std::vector<double> xd(std::max(cols, 1)), yd(std::max(rows, 1));
+    for (int j = 0; j < cols; ++j) xd[j] = x[in_perm[j]];
+    double *dx = nullptr, *dy = nullptr;
+    cuda_ok(cudaMalloc(&dx, xd.size() * sizeof(double)), "cudaMalloc");
+    cuda_ok(cudaMalloc(&dy, yd.size() * sizeof(double)), "cudaMalloc");
+    cuda_ok(cudaMemcpy(dx, xd.data(), xd.size() * sizeof(double), cudaMemcpyHostToDevice), "H2D");
+    if (S.n_slices > 0) {
+        if (exact32) dev::k_spmv<double, float, double><<<std::max(1, S.n_slices / 8 + 1), 256, 0, stream>>>(S, dx, dy);
+        else dev::k_spmv<double, double, double><<<std::max(1, S.n_slices / 8 + 1), 256, 0, stream>>>(S, dx, dy);
+    }
+    cuda_ok(cudaGetLastError(), "k_spmv");
+    cuda_ok(cudaStreamSynchronize(stream), "k_spmv");
+    cuda_ok(cudaMemcpy(yd.data(), dy, yd.size() * sizeof(double), cudaMemcpyDeviceToHost), "D2H");
+    cudaFree(dx);
+    cudaFree(dy);
+    for (int r = 0; r < rows; ++r) y[out_perm[r]] = yd[r];
+}
 
 BatchImpl* batch_create(int n, const b2_lp_view* U, const b2_lp_view* S, const double* const* Dr,
                         const double* const* Dc, const b2_solve_opts& o) {

@@ -51,6 +51,10 @@ struct b2_batch {
     b2::BatchImpl* impl;
 };
 
+struct b2_server {
+    b2::ServerImpl* impl;
+};
+
 extern "C" {
 
 void b2_default_opts(b2_solve_opts* o) {
@@ -160,6 +164,53 @@ int b2_engine_trace(b2_engine* e, double* out, int32_t max_records, int32_t* cou
         if (!e || !count) b2::fail(B2_ERR_INVALID, "null argument");
         *count = b2::engine_trace(e->impl, out, max_records);
     });
+}
+
+int b2_server_create(const b2_server_opts* sopts, const b2_solve_opts* opts, b2_server** out) {
+    return b2::guarded([&] {
+        if (!out) b2::fail(B2_ERR_INVALID, "null argument");
+        *out = nullptr;
+        b2_server_opts so;
+        std::memset(&so, 0, sizeof(so));
+        if (sopts) so = *sopts;
+        b2_solve_opts o;
+        if (opts) o = *opts;
+        else b2_default_opts(&o);
+        b2::ServerImpl* s = b2::server_create(so, o);
+        *out = new b2_server{s};
+    });
+}
+
+int b2_server_submit(b2_server* s, const b2_lp_view* U, int64_t* ticket) {
+    return b2::guarded([&] {
+        if (!s || !U || !ticket) b2::fail(B2_ERR_INVALID, "null argument");
+        *ticket = b2::server_submit(s->impl, *U);
+    });
+}
+
+int b2_server_wait(b2_server* s, int64_t ticket, double timeout_s, double* x, double* y, b2_result* res,
+                   b2_request_info* info) {
+    int rc = B2_OK;
+    const int g = b2::guarded([&] {
+        if (!s) b2::fail(B2_ERR_INVALID, "null argument");
+        rc = b2::server_wait(s->impl, ticket, timeout_s, x, y, res, info);
+    });
+    if (g != B2_OK) return g;
+    if (rc == B2_ERR_PENDING) b2::set_last_error("request not finished yet");
+    return rc;
+}
+
+int b2_server_stats_get(b2_server* s, b2_server_stats* out) {
+    return b2::guarded([&] {
+        if (!s || !out) b2::fail(B2_ERR_INVALID, "null argument");
+        b2::server_stats(s->impl, out);
+    });
+}
+
+void b2_server_destroy(b2_server* s) {
+    if (!s) return;
+    b2::server_destroy(s->impl);
+    delete s;
 }
 
 int b2_batch_create(int32_t n_lp, const b2_lp_view* U, const b2_lp_view* S, const double* const* Dr,

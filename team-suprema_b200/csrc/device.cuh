@@ -50,7 +50,10 @@ constexpr int kPartStride = 32;  // doubles per CTA per reduction slot
 constexpr int kMaxNV = 22;
 enum { SLOT_A = 0, SLOT_X = 1, SLOT_CK = 2, NSLOTS = 3 };
 enum { SEL_BEST = 0, SEL_CUR = 1, SEL_AVG = 2 };
-enum { MODE_START = 0, MODE_RESUME = 1 };
+// MODE_START: cold start. MODE_RESUME: the FP64 phase takes over from the
+// FP32 phase (iterates widened, A x / A^T y recomputed). MODE_CONTINUE: the
+// same phase goes on after a yield, from exactly the state it left.
+enum { MODE_START = 0, MODE_RESUME = 1, MODE_CONTINUE = 2 };
 // Group kinds: one CTA (barrier __syncthreads, partial sums in shared memory,
 // iterates read through L1), a thread-block cluster (hardware cluster
 // barrier), the whole grid of a cooperative launch (software grid barrier).
@@ -70,6 +73,12 @@ struct SellDev {
     const uint32_t* col;
     const float* v32;
     const double* v64;
+    // split slices (long rows, whole-GPU engine only): per split group
+    // {segments, first partial slot}, the partial sums (32 per segment) and
+    // one arrival counter per group, zero between products
+    const int2* seg;
+    double* seg_part;
+    unsigned* seg_cnt;
 };
 
 template <class T>
@@ -93,6 +102,11 @@ struct Ctl {
     int last_accepted, best_valid, stall, exit_reason, out_sel;
     int mode, check_now, switch_req, stop_req;
     int fp32_attempts, fp32_accepted;
+    // yield / continue (rounds of a served batch): the phase the LP is in
+    // (1: FP64 iterates), a pending yield, and the group total of |dx|^2 of
+    // the primal step already taken for the next attempt
+    int phase64, yield_req;
+    double dx2_carry;
 };
 
 // Pointers and constants of one LP (independent of the iterate precision).
@@ -118,6 +132,22 @@ struct KParams : KParamsBase {
     Bufs<T> it;  // iterates at this precision
 };
 
+// Every device pointer and constant of one LP, for kernels that take LPs from
+// a work queue (batches, served rounds): the LP may live in its own device
+// region or at offsets inside shared pools.
+struct LpDev {
+    int m, n;
+    SellDev A, AT;
+    const double *b, *rU, *dr2, *c, *l, *u, *dc2, *x0;
+    const int32_t *perm_r, *perm_c;
+    Bufs<float> itf;
+    Bufs<double> itd;
+    double *xsum, *ysum, *best_x, *best_y, *out_x, *out_y;
+    Ctl* ctl;
+    double denom_p, denom_d;
+    int exact32, pad;
+};
+
 // The CTAs that cooperate on one LP, and this CTA's place in them.
 struct Group {
     int rank, size;          // this CTA's index, number of CTAs
@@ -128,6 +158,13 @@ struct Group {
     int* abort;
     unsigned long long timeout_ns;
     double* spart;           // GK_CTA: partial sums in shared memory, [NSLOTS][kPartStride]
+    // global-timer deadline after which the solve yields at the next attempt
+    // boundary (read on the group's first CTA only); 0: never
+    unsigned long long yield_at = 0;
+    // GK_CTA: shared memory for the two gathered iterates (x' for A x', y'
+    // for A^T y'), used when both fit; null: gathers read global memory
+    unsigned char* svec = nullptr;
+    int svec_bytes = 0;
 };
 
 // ------------------------------------------------------------- primitives
@@ -292,6 +329,11 @@ __device__ __forceinline__ void step_totals(const Group& g, double* s_tot) {
 // One slice of a sliced-ELL matrix times a gathered vector: every lane sums
 // its share of its row in a fixed order, then the g lanes of a row are
 // folded onto the row's first lane (fixed tree).
+#ifndef B2_SLICE_UNROLL
+#define B2_SLICE_UNROLL 4
+#endif
+constexpr int kUnroll = B2_SLICE_UNROLL;
+
 template <int GK, class AccT, class V, class XT>
 __device__ __forceinline__ AccT slice_dot(const SellDev& S, const V* vbase, int4 sl, int lane, const XT* x) {
     const uint32_t len = (uint32_t)sl.y & kLenMask;
@@ -301,17 +343,23 @@ __device__ __forceinline__ AccT slice_dot(const SellDev& S, const V* vbase, int4
     const V* vp = vbase + base;
     AccT acc = AccT(0);
     uint32_t k = 0;
-    for (; k + 4 <= len; k += 4) {
-        const uint32_t c0 = ld_mat(cp), c1 = ld_mat(cp + 32), c2 = ld_mat(cp + 64), c3 = ld_mat(cp + 96);
-        const V v0 = ld_mat(vp), v1 = ld_mat(vp + 32), v2 = ld_mat(vp + 64), v3 = ld_mat(vp + 96);
-        const AccT x0 = (AccT)ld_it<GK>(x + c0), x1 = (AccT)ld_it<GK>(x + c1), x2 = (AccT)ld_it<GK>(x + c2),
-                   x3 = (AccT)ld_it<GK>(x + c3);
-        acc = fma((AccT)v0, x0, acc);
-        acc = fma((AccT)v1, x1, acc);
-        acc = fma((AccT)v2, x2, acc);
-        acc = fma((AccT)v3, x3, acc);
-        cp += 128;
-        vp += 128;
+    // kUnroll gathers in flight per lane; the sum stays one sequential fma
+    // chain, so the unroll depth never changes the result
+    for (; k + kUnroll <= len; k += kUnroll) {
+        uint32_t cc[kUnroll];
+        V vv[kUnroll];
+        AccT xx[kUnroll];
+#pragma unroll
+        for (int q = 0; q < kUnroll; ++q) {
+            cc[q] = ld_mat(cp + 32 * q);
+            vv[q] = ld_mat(vp + 32 * q);
+        }
+#pragma unroll
+        for (int q = 0; q < kUnroll; ++q) xx[q] = (AccT)ld_it<GK>(x + cc[q]);
+#pragma unroll
+        for (int q = 0; q < kUnroll; ++q) acc = fma((AccT)vv[q], xx[q], acc);
+        cp += 32 * kUnroll;
+        vp += 32 * kUnroll;
     }
     for (; k < len; ++k) {
         acc = fma((AccT)ld_mat(vp), (AccT)ld_it<GK>(x + ld_mat(cp)), acc);
@@ -320,6 +368,39 @@ __device__ __forceinline__ AccT slice_dot(const SellDev& S, const V* vbase, int4
     }
     for (int o = (1 << lg) >> 1; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
     return acc;
+}
+
+// A split slice is one of `segments` consecutive slice records over the same
+// rows, each covering a range of steps (slice.w = group + 1 | segment << 24;
+// 0 for an unsplit slice). Every segment publishes its lanes' partial sums;
+// the warp that completes the group adds them in segment order (the result
+// does not depend on which warp that is) and alone goes on to the row's
+// epilogue. Returns whether this warp holds complete row sums in `acc`.
+template <int GK, class AccT>
+__device__ __forceinline__ bool seg_finish(const SellDev& S, int4 sl, int lane, AccT& acc) {
+    if (GK != GK_GRID || sl.w == 0) return true;  // only the whole-GPU layout splits slices
+    const int grp = (sl.w & 0xFFFFFF) - 1, q = (int)((unsigned)sl.w >> 24);
+    const int2 info = __ldg(S.seg + grp);
+    double* part = S.seg_part + (size_t)info.y * 32;
+    __stcg(part + q * 32 + lane, (double)acc);
+    __threadfence();
+    __syncwarp();
+    unsigned last = 0;
+    if (lane == 0) last = atomicAdd(S.seg_cnt + grp, 1u) == (unsigned)(info.x - 1) ? 1u : 0u;
+    last = __shfl_sync(0xffffffffu, last, 0);
+    if (!last) return false;
+    __threadfence();
+    AccT tot = AccT(0);
+    for (int t = 0; t < info.x; ++t) tot += (AccT)__ldcg(part + t * 32 + lane);
+    acc = tot;
+    if (lane == 0) S.seg_cnt[grp] = 0u;  // the next product over this matrix comes after a barrier
+    return true;
+}
+// A pass that needs no product over a split slice still runs the row's
+// epilogue once: in the warp of segment 0.
+template <int GK>
+__device__ __forceinline__ bool seg_first(int4 sl) {
+    return GK != GK_GRID || sl.w == 0 || ((unsigned)sl.w >> 24) == 0u;
 }
 
 // verify.cpp:35-87 terms of one row: row violation^2, sign violation^2,
@@ -368,12 +449,13 @@ __device__ __forceinline__ void kkt_col(double l, double u, double cc, double x,
 // unscaled coordinates: x' = clamp(x - tau Dc^2 (c - A^T y), l, u).
 template <class T>
 __device__ __forceinline__ void primal_col(const KParams<T>& P, int j, T xv, double g, double tau, T* xn,
-                                           double& dx2) {
+                                           double& dx2, T* xs) {
     const double w = __ldg(P.dc2 + j);
     double v = (double)xv - tau * w * (__ldg(P.c + j) - g);
     v = fmin(fmax(v, __ldg(P.l + j)), __ldg(P.u + j));
     const T vt = (T)v;
     xn[j] = vt;
+    if (xs) xs[j] = vt;  // the copy the next A x' gathers from
     const double d = (double)vt - (double)xv;
     dx2 += d * d / w;
 }
@@ -383,8 +465,9 @@ __device__ __forceinline__ void primal_col(const KParams<T>& P, int j, T xv, dou
 // Rows: A x' fused with the dual step (pdlp_algo.hpp:111-112, src/pdlp.cpp:125-130)
 // and the step-size statistics (pdlp_gpu_solve.cu:119-131).
 template <int GK, class T, class V>
-__device__ void pass_rows_step(const KParams<T>& P, const Ctl& c, const Group& g, int lane, double* v) {
-    const T* xn = P.it.x[1 - c.xi];
+__device__ void pass_rows_step(const KParams<T>& P, const Ctl& c, const Group& g, int lane, double* v, T* sx,
+                               T* sy) {
+    const T* xn = sx ? sx : P.it.x[1 - c.xi];
     const T* y = P.it.y[c.yi];
     T* yn = P.it.y[1 - c.yi];
     const T* ax = P.it.ax[c.ax_cur];
@@ -393,7 +476,8 @@ __device__ void pass_rows_step(const KParams<T>& P, const Ctl& c, const Group& g
     const V* vb = vals<V>(P.A);
     for (int s = g.gw; s < P.A.n_slices; s += g.nw) {
         const int4 sl = __ldg(P.A.slice + s);
-        const T acc = slice_dot<GK, T, V, T>(P.A, vb, sl, lane, xn);
+        T acc = slice_dot<GK, T, V, T>(P.A, vb, sl, lane, xn);
+        if (!seg_finish<GK, T>(P.A, sl, lane, acc)) continue;
         const int lg = (int)((uint32_t)sl.y >> kLenBits);
         const int row = sl.x + (lane >> lg);
         if ((lane & ((1 << lg) - 1)) == 0 && row < P.m) {
@@ -404,6 +488,7 @@ __device__ void pass_rows_step(const KParams<T>& P, const Ctl& c, const Group& g
             if (w < 0.0 && nv < 0.0) nv = 0.0;
             const T nt = (T)nv;
             yn[row] = nt;
+            if (sy) sy[row] = nt;
             axn[row] = acc;
             const double d = (double)nt - (double)yv;
             v[0] += d * d / aw;
@@ -415,29 +500,31 @@ __device__ void pass_rows_step(const KParams<T>& P, const Ctl& c, const Group& g
 
 // Columns: [accepted] A^T y' + x-average update, then the next primal step.
 template <int GK, class T, class V>
-__device__ void pass_cols_step(const KParams<T>& P, const Ctl& c, const Group& g, int lane, double& dx2) {
+__device__ void pass_cols_step(const KParams<T>& P, const Ctl& c, const Group& g, int lane, double& dx2, T* sx,
+                               const T* sy) {
     const T* x = P.it.x[c.xi];
     T* xn = P.it.x[1 - c.xi];
     T* aty = P.it.aty[c.aty_cur];
     const double tau = c.eta / c.omega, pend = c.pend_x;
     if (c.last_accepted) {
-        const T* y = P.it.y[c.yi];
+        const T* y = sy ? sy : P.it.y[c.yi];
         const V* vb = vals<V>(P.AT);
         for (int s = g.gw; s < P.AT.n_slices; s += g.nw) {
             const int4 sl = __ldg(P.AT.slice + s);
-            const T acc = slice_dot<GK, T, V, T>(P.AT, vb, sl, lane, y);
+            T acc = slice_dot<GK, T, V, T>(P.AT, vb, sl, lane, y);
+            if (!seg_finish<GK, T>(P.AT, sl, lane, acc)) continue;
             const int lg = (int)((uint32_t)sl.y >> kLenBits);
             const int j = sl.x + (lane >> lg);
             if ((lane & ((1 << lg) - 1)) == 0 && j < P.n) {
                 aty[j] = acc;
                 const T xv = ld_it<GK>(x + j);
                 if (pend != 0.0) P.xsum[j] += pend * (double)xv;
-                primal_col<T>(P, j, xv, (double)acc, tau, xn, dx2);
+                primal_col<T>(P, j, xv, (double)acc, tau, xn, dx2, sx);
             }
         }
     } else {
         for (int j = g.gt; j < P.n; j += g.nt)
-            primal_col<T>(P, j, ld_it<GK>(x + j), (double)ld_it<GK>(aty + j), tau, xn, dx2);
+            primal_col<T>(P, j, ld_it<GK>(x + j), (double)ld_it<GK>(aty + j), tau, xn, dx2, sx);
     }
 }
 
@@ -455,7 +542,12 @@ __device__ void pass_rows_check(const KParams<T>& P, const Ctl& c, const Group& 
     for (int s = g.gw; s < P.A.n_slices; s += g.nw) {
         const int4 sl = __ldg(P.A.slice + s);
         double acc = 0.0;
-        if (has_avg) acc = slice_dot<GK, double, V, double>(P.A, vb, sl, lane, P.xsum);
+        if (has_avg) {
+            acc = slice_dot<GK, double, V, double>(P.A, vb, sl, lane, P.xsum);
+            if (!seg_finish<GK, double>(P.A, sl, lane, acc)) continue;
+        } else if (!seg_first<GK>(sl)) {
+            continue;
+        }
         const int lg = (int)((uint32_t)sl.y >> kLenBits);
         const int i = sl.x + (lane >> lg);
         if ((lane & ((1 << lg) - 1)) == 0 && i < P.m) {
@@ -487,7 +579,12 @@ __device__ void pass_cols_check(const KParams<T>& P, const Ctl& c, const Group& 
     for (int s = g.gw; s < P.AT.n_slices; s += g.nw) {
         const int4 sl = __ldg(P.AT.slice + s);
         double acc = 0.0;
-        if (has_avg) acc = slice_dot<GK, double, V, double>(P.AT, vb, sl, lane, P.ysum);
+        if (has_avg) {
+            acc = slice_dot<GK, double, V, double>(P.AT, vb, sl, lane, P.ysum);
+            if (!seg_finish<GK, double>(P.AT, sl, lane, acc)) continue;
+        } else if (!seg_first<GK>(sl)) {
+            continue;
+        }
         const int lg = (int)((uint32_t)sl.y >> kLenBits);
         const int j = sl.x + (lane >> lg);
         if ((lane & ((1 << lg) - 1)) == 0 && j < P.n) {
@@ -509,7 +606,7 @@ __device__ void pass_cols_check(const KParams<T>& P, const Ctl& c, const Group& 
 // and, on restart, redo the next primal step with the new primal weight.
 template <int GK, class T>
 __device__ void pass_after_check(const KParams<T>& P, const Ctl& c, const Group& g, int best_sel, int restart,
-                                 int use_avg, double wsum_old, double& dx2) {
+                                 int use_avg, double wsum_old, double& dx2, T* sx) {
     const bool has_avg = wsum_old > 0;
     T* x = P.it.x[c.xi];
     T* xn = P.it.x[1 - c.xi];
@@ -527,7 +624,7 @@ __device__ void pass_after_check(const KParams<T>& P, const Ctl& c, const Group&
             if (use_avg) { xnew = (T)xa; x[j] = xnew; }
             P.xsum[j] = 0.0;
             const double gg = (double)ld_it<GK>((use_avg ? P.it.aty[c.aty_avg] : P.it.aty[c.aty_cur]) + j);
-            primal_col<T>(P, j, xnew, gg, tau, xn, dx2);
+            primal_col<T>(P, j, xnew, gg, tau, xn, dx2, sx);
         }
     }
     T* y = P.it.y[c.yi];
@@ -660,6 +757,35 @@ __device__ bool run_check(const KParams<T>& P, Ctl& s, const Group& g, int lane,
     return true;
 }
 
+// Yield at an attempt boundary (after the columns pass and its barrier, or
+// after a KKT check): the next attempt's primal step is taken, its |dx|^2
+// partials wait in the group's scratch, everything else is in P's buffers
+// and the control state. The group total of those partials is formed exactly
+// as step_totals forms it and kept in the control state, which the group's
+// first CTA writes back with mode MODE_CONTINUE.
+template <int GK>
+__device__ bool yield_state(const KParamsBase& P, Ctl& s, const Group& g) {
+    __shared__ double s_carry;
+    if (GK == GK_CTA) {
+        if (threadIdx.x == 0) s_carry = g.spart[SLOT_X * kPartStride];
+    } else if (threadIdx.x < 32) {
+        double v = 0.0;
+        for (int b = threadIdx.x; b < g.size; b += 32) v += __ldcg(&g.part[((size_t)SLOT_X * g.size + b) * kPartStride]);
+        v = warp_total(v);
+        if (threadIdx.x == 0) s_carry = v;
+    }
+    __syncthreads();
+    if (g.rank == 0 && threadIdx.x == 0) {
+        s.dx2_carry = s_carry;
+        s.mode = MODE_CONTINUE;
+        s.yield_req = 0;
+        s.check_now = 0;
+        *P.ctl = s;
+    }
+    __syncthreads();
+    return true;
+}
+
 // ------------------------------------------------------------ the solve
 //
 // Per attempt:   rows pass -> barrier -> step decision -> cols pass -> barrier
@@ -668,7 +794,7 @@ __device__ bool run_check(const KParams<T>& P, Ctl& s, const Group& g, int lane,
 // The group's CTAs enter with the same P and leave together. The control
 // state is read from P.ctl at entry and written back by the group's first CTA
 // at exit. Returns false when a barrier wait timed out (abort).
-template <int GK, class T, class V>
+template <int GK, class T, class V, bool STAGE = false>
 __device__ bool solve_body(const KParams<T>& P, const Group& g) {
     __shared__ Ctl s;
     __shared__ double s_red[kWarps * kMaxNV];
@@ -680,73 +806,101 @@ __device__ bool solve_body(const KParams<T>& P, const Group& g) {
 
     if (tid == 0) s = *P.ctl;
     __syncthreads();
-    const bool first_check = s.check_now != 0;
-    if (g.rank == 0 && tid == 0 && s.mode == MODE_START) g.bcast[2] = (double)gtimer();
+    const bool first_check = s.check_now != 0 && s.mode != MODE_CONTINUE;
+    const bool ypoll = g.yield_at != 0;
+    if (g.rank == 0 && tid == 0 && s.mode == MODE_START) s.t_start = (double)gtimer();
+    // one CTA alone on the GPU (STAGE): x' and y' also live in shared memory
+    // when they fit, and the SpMV gathers read them there (same values, same
+    // order). Kernels that keep several CTAs per SM leave it off: the shared
+    // memory would come out of the L1 that already caches their iterates.
+    T* sx = nullptr;
+    T* sy = nullptr;
+    if (STAGE && GK == GK_CTA && g.svec && ((size_t)P.n + (size_t)P.m) * sizeof(T) <= (size_t)g.svec_bytes) {
+        sx = reinterpret_cast<T*>(g.svec);
+        sy = sx + P.n;
+    }
 
     // ---------------------------------------------------------- start-up
-    if (s.mode == MODE_START) {
-        // x = x0, y = 0, A^T y = 0, sums = 0 (pdlp_algo.hpp:68-84)
-        for (int j = g.gt; j < P.n; j += g.nt) {
-            const T x0 = (T)__ldg(P.x0 + j);
-            P.it.x[s.xi][j] = x0;
-            P.it.x_last[j] = x0;
-            P.it.aty[s.aty_cur][j] = T(0);
-            P.xsum[j] = 0.0;
+    if (s.mode == MODE_CONTINUE) {
+        // after a yield: every iterate, A x, A^T y and the primal step of the
+        // next attempt are where the yield left them; only the |dx|^2 partial
+        // sums lived in the group's scratch. Put back the group total as rank
+        // 0's partial and zeros for the others: the totals below then come
+        // out bit-identical to the ones the uninterrupted solve would form.
+        if (tid == 0) {
+            if (GK == GK_CTA) g.spart[SLOT_X * kPartStride] = s.dx2_carry;
+            else g.part[((size_t)SLOT_X * g.size + g.rank) * kPartStride] = g.rank == 0 ? s.dx2_carry : 0.0;
         }
-        for (int i = g.gt; i < P.m; i += g.nt) {
-            P.it.y[s.yi][i] = T(0);
-            P.it.y_last[i] = T(0);
-            P.ysum[i] = 0.0;
-        }
+        if (sx)
+            for (int j = g.gt; j < P.n; j += g.nt) sx[j] = ld_it<GK>(P.it.x[1 - s.xi] + j);
+        __syncthreads();
     } else {
-        // resume with FP64 iterates after the FP32 phase
-        for (int j = g.gt; j < P.n; j += g.nt) {
-            P.it.x[s.xi][j] = (T)P.itf.x[s.xi][j];
-            P.it.x_last[j] = (T)P.itf.x_last[j];
-        }
-        for (int i = g.gt; i < P.m; i += g.nt) {
-            P.it.y[s.yi][i] = (T)P.itf.y[s.yi][i];
-            P.it.y_last[i] = (T)P.itf.y_last[i];
-        }
-    }
-    if (P.debug_delay_ns && g.rank == 0 && tid == 0) {
-        // test hook (bounded): hold the first CTA back so the others' barrier wait runs out
-        const unsigned long long t0 = gtimer();
-        while (gtimer() - t0 < P.debug_delay_ns) __nanosleep(1000);
-    }
-    if (!group_sync<GK>(g)) return false;
-    {   // A x (and A^T y when resuming) at this precision
-        const V* vb = vals<V>(P.A);
-        T* ax = P.it.ax[s.ax_cur];
-        for (int k = g.gw; k < P.A.n_slices; k += g.nw) {
-            const int4 sl = __ldg(P.A.slice + k);
-            const T acc = slice_dot<GK, T, V, T>(P.A, vb, sl, lane, P.it.x[s.xi]);
-            const int lg = (int)((uint32_t)sl.y >> kLenBits);
-            const int i = sl.x + (lane >> lg);
-            if ((lane & ((1 << lg) - 1)) == 0 && i < P.m) ax[i] = acc;
-        }
-        if (s.mode == MODE_RESUME) {
-            const V* vt = vals<V>(P.AT);
-            T* aty = P.it.aty[s.aty_cur];
-            for (int k = g.gw; k < P.AT.n_slices; k += g.nw) {
-                const int4 sl = __ldg(P.AT.slice + k);
-                const T acc = slice_dot<GK, T, V, T>(P.AT, vt, sl, lane, P.it.y[s.yi]);
-                const int lg = (int)((uint32_t)sl.y >> kLenBits);
-                const int j = sl.x + (lane >> lg);
-                if ((lane & ((1 << lg) - 1)) == 0 && j < P.n) aty[j] = acc;
+        if (s.mode == MODE_START) {
+            // x = x0, y = 0, A^T y = 0, sums = 0 (pdlp_algo.hpp:68-84)
+            for (int j = g.gt; j < P.n; j += g.nt) {
+                const T x0 = (T)__ldg(P.x0 + j);
+                P.it.x[s.xi][j] = x0;
+                P.it.x_last[j] = x0;
+                P.it.aty[s.aty_cur][j] = T(0);
+                P.xsum[j] = 0.0;
+            }
+            for (int i = g.gt; i < P.m; i += g.nt) {
+                P.it.y[s.yi][i] = T(0);
+                P.it.y_last[i] = T(0);
+                P.ysum[i] = 0.0;
+            }
+        } else {
+            // resume with FP64 iterates after the FP32 phase
+            for (int j = g.gt; j < P.n; j += g.nt) {
+                P.it.x[s.xi][j] = (T)P.itf.x[s.xi][j];
+                P.it.x_last[j] = (T)P.itf.x_last[j];
+            }
+            for (int i = g.gt; i < P.m; i += g.nt) {
+                P.it.y[s.yi][i] = (T)P.itf.y[s.yi][i];
+                P.it.y_last[i] = (T)P.itf.y_last[i];
             }
         }
+        if (P.debug_delay_ns && g.rank == 0 && tid == 0) {
+            // test hook (bounded): hold the first CTA back so the others' barrier wait runs out
+            const unsigned long long t0 = gtimer();
+            while (gtimer() - t0 < P.debug_delay_ns) __nanosleep(1000);
+        }
+        if (!group_sync<GK>(g)) return false;
+        {   // A x (and A^T y when resuming) at this precision
+            const V* vb = vals<V>(P.A);
+            T* ax = P.it.ax[s.ax_cur];
+            for (int k = g.gw; k < P.A.n_slices; k += g.nw) {
+                const int4 sl = __ldg(P.A.slice + k);
+                T acc = slice_dot<GK, T, V, T>(P.A, vb, sl, lane, P.it.x[s.xi]);
+                if (!seg_finish<GK, T>(P.A, sl, lane, acc)) continue;
+                const int lg = (int)((uint32_t)sl.y >> kLenBits);
+                const int i = sl.x + (lane >> lg);
+                if ((lane & ((1 << lg) - 1)) == 0 && i < P.m) ax[i] = acc;
+            }
+            if (s.mode == MODE_RESUME) {
+                const V* vt = vals<V>(P.AT);
+                T* aty = P.it.aty[s.aty_cur];
+                for (int k = g.gw; k < P.AT.n_slices; k += g.nw) {
+                    const int4 sl = __ldg(P.AT.slice + k);
+                    T acc = slice_dot<GK, T, V, T>(P.AT, vt, sl, lane, P.it.y[s.yi]);
+                    if (!seg_finish<GK, T>(P.AT, sl, lane, acc)) continue;
+                    const int lg = (int)((uint32_t)sl.y >> kLenBits);
+                    const int j = sl.x + (lane >> lg);
+                    if ((lane & ((1 << lg) - 1)) == 0 && j < P.n) aty[j] = acc;
+                }
+            }
+        }
+        if (!group_sync<GK>(g)) return false;
+        {   // primal step of the first attempt
+            double dx2[1] = {0.0};
+            const double tau = s.eta / s.omega;
+            for (int j = g.gt; j < P.n; j += g.nt)
+                primal_col<T>(P, j, ld_it<GK>(P.it.x[s.xi] + j), (double)ld_it<GK>(P.it.aty[s.aty_cur] + j), tau,
+                              P.it.x[1 - s.xi], dx2[0], sx);
+            cta_partial<1, GK>(dx2, g, SLOT_X, s_red);
+        }
+        if (!group_sync<GK>(g)) return false;
     }
-    if (!group_sync<GK>(g)) return false;
-    {   // primal step of the first attempt
-        double dx2[1] = {0.0};
-        const double tau = s.eta / s.omega;
-        for (int j = g.gt; j < P.n; j += g.nt)
-            primal_col<T>(P, j, ld_it<GK>(P.it.x[s.xi] + j), (double)ld_it<GK>(P.it.aty[s.aty_cur] + j), tau,
-                          P.it.x[1 - s.xi], dx2[0]);
-        cta_partial<1, GK>(dx2, g, SLOT_X, s_red);
-    }
-    if (!group_sync<GK>(g)) return false;
 
     // --------------------------------------------------------- main loop
     bool check_pending = first_check;
@@ -758,12 +912,15 @@ __device__ bool solve_body(const KParams<T>& P, const Group& g) {
             if (poll && g.rank == 0 && tid == 0 && P.host_stop) hstop = *P.host_stop;
             {
                 double v[2] = {0.0, 0.0};
-                pass_rows_step<GK, T, V>(P, s, g, lane, v);
+                pass_rows_step<GK, T, V>(P, s, g, lane, v, sx, sy);
                 cta_partial<2, GK>(v, g, SLOT_A, s_red);
             }
-            if (poll && g.rank == 0 && tid == 0) {
-                g.bcast[0] = (double)hstop;
-                g.bcast[1] = (P.time_limit_ns > 0 && (double)gtimer() - g.bcast[2] > P.time_limit_ns) ? 1.0 : 0.0;
+            if (g.rank == 0 && tid == 0) {
+                if (poll) {
+                    g.bcast[0] = (double)hstop;
+                    g.bcast[1] = (P.time_limit_ns > 0 && (double)gtimer() - s.t_start > P.time_limit_ns) ? 1.0 : 0.0;
+                }
+                if (ypoll) g.bcast[3] = gtimer() >= g.yield_at ? 1.0 : 0.0;
             }
             if (!group_sync<GK>(g)) return false;
             step_totals<GK>(g, s_tot);
@@ -798,6 +955,7 @@ __device__ bool solve_body(const KParams<T>& P, const Group& g) {
                     if (__ldcg(&g.bcast[0]) != 0.0) s.stop_req = B2_EXIT_STOPPED;
                     else if (__ldcg(&g.bcast[1]) != 0.0) s.stop_req = B2_EXIT_TIME_LIMIT;
                 }
+                if (ypoll && __ldcg(&g.bcast[3]) != 0.0) s.yield_req = 1;
                 s_flag[0] = (s.last_accepted && (s.accepted % P.check_every) == 0) || s.attempts >= P.max_iterations;
             }
             __syncthreads();
@@ -805,7 +963,7 @@ __device__ bool solve_body(const KParams<T>& P, const Group& g) {
             // ---- cols pass: A^T y' (if accepted) + next primal step ----
             {
                 double dx2[1] = {0.0};
-                pass_cols_step<GK, T, V>(P, s, g, lane, dx2[0]);
+                pass_cols_step<GK, T, V>(P, s, g, lane, dx2[0], sx, sy);
                 cta_partial<1, GK>(dx2, g, SLOT_X, s_red);
             }
             if (tid == 0) {
@@ -815,6 +973,7 @@ __device__ bool solve_body(const KParams<T>& P, const Group& g) {
             if (!group_sync<GK>(g)) return false;
             if (!check_due) {
                 if (s.exit_reason != 0) break;
+                if (s.yield_req) return yield_state<GK>(P, s, g);
                 continue;
             }
         }
@@ -827,7 +986,7 @@ __device__ bool solve_body(const KParams<T>& P, const Group& g) {
             const int best_sel = s_flag[0], restart = s_flag[1], use_avg = s_flag[2];
             if (best_sel != 0 || restart) {
                 double dx2[1] = {0.0};
-                pass_after_check<GK, T>(P, s, g, best_sel, restart, use_avg, s_wsum_old, dx2[0]);
+                pass_after_check<GK, T>(P, s, g, best_sel, restart, use_avg, s_wsum_old, dx2[0], sx);
                 if (restart) cta_partial<1, GK>(dx2, g, SLOT_X, s_red);
                 __syncthreads();
                 if (tid == 0 && restart && use_avg) {
@@ -838,6 +997,7 @@ __device__ bool solve_body(const KParams<T>& P, const Group& g) {
             }
         }
         if (s.switch_req || s.exit_reason != 0) break;
+        if (s.yield_req) return yield_state<GK>(P, s, g);
     }
 
     // ------------------------------------------------------------- exit
@@ -888,7 +1048,8 @@ __global__ void __launch_bounds__(256) k_spmv(SellDev S, const XT* x, AccT* y) {
     const V* vb = vals<V>(S);
     for (int s = gw; s < S.n_slices; s += nw) {
         const int4 sl = __ldg(S.slice + s);
-        const AccT acc = slice_dot<GK_GRID, AccT, V, XT>(S, vb, sl, lane, x);
+        AccT acc = slice_dot<GK_GRID, AccT, V, XT>(S, vb, sl, lane, x);
+        if (!seg_finish<GK_GRID, AccT>(S, sl, lane, acc)) continue;
         const int lg = (int)((uint32_t)sl.y >> kLenBits);
         const int r = sl.x + (lane >> lg);
         if ((lane & ((1 << lg) - 1)) == 0 && r < S.n_rows) y[r] = acc;

@@ -14,7 +14,7 @@
 #include <string>
 #include <vector>
 
-#include "device.cuh"
+#include "batch.h"
 
 namespace b2 {
 namespace dev {
@@ -26,6 +26,8 @@ struct GridArgs {
     unsigned* bar;
     int* abort;
     unsigned long long timeout_ns;
+    unsigned long long yield_ns;  // the solve yields this long after the launch starts; 0: never
+    int svec_bytes;               // one-CTA launch: dynamic shared memory for staged x' / y'
 };
 
 template <class T, class V>
@@ -43,6 +45,7 @@ __global__ void __launch_bounds__(kBlock, 2) k_pdlp(const KParams<T> P, const Gr
     g.abort = ga.abort;
     g.timeout_ns = ga.timeout_ns;
     g.spart = nullptr;
+    if (ga.yield_ns) g.yield_at = gtimer() + ga.yield_ns;  // read on CTA 0 only
     solve_body<GK_GRID, T, V>(P, g);
 }
 
@@ -51,6 +54,7 @@ __global__ void __launch_bounds__(kBlock, 2) k_pdlp(const KParams<T> P, const Gr
 template <class T, class V>
 __global__ void __launch_bounds__(kBlock, 2) k_pdlp_cta(const KParams<T> P, const GridArgs ga) {
     __shared__ double s_part[NSLOTS * kPartStride];
+    extern __shared__ __align__(16) unsigned char s_vec[];
     Group g;
     g.rank = 0;
     g.size = 1;
@@ -64,7 +68,10 @@ __global__ void __launch_bounds__(kBlock, 2) k_pdlp_cta(const KParams<T> P, cons
     g.abort = ga.abort;
     g.timeout_ns = 0;
     g.spart = s_part;
-    solve_body<GK_CTA, T, V>(P, g);
+    if (ga.yield_ns) g.yield_at = gtimer() + ga.yield_ns;
+    g.svec = ga.svec_bytes > 0 ? s_vec : nullptr;
+    g.svec_bytes = ga.svec_bytes;
+    solve_body<GK_CTA, T, V, true>(P, g);
 }
 
 }  // namespace dev
@@ -142,6 +149,13 @@ struct EngineImpl {
         d.col = up(S.col);
         d.v32 = up(S.val32);
         d.v64 = S.val64.empty() ? nullptr : up(S.val64);
+        if (S.n_groups() > 0) {
+            d.seg = reinterpret_cast<const int2*>(up(S.seg));
+            d.seg_part = alloc<double>((size_t)S.seg_slots * 32);
+            unsigned* cnt = alloc<unsigned>((size_t)S.n_groups());
+            cuda_ok(cudaMemset(cnt, 0, sizeof(unsigned) * (size_t)S.n_groups()), "memset");
+            d.seg_cnt = cnt;
+        }
         return d;
     }
 
@@ -162,7 +176,12 @@ struct EngineImpl {
         BuildParams bp;
         bp.lane_target = o.lane_target;
         bp.sigma_window = o.sigma_window;
+        bp.split = true;  // the whole GPU works on this LP: tune and split long rows
         build_layout(U, S, Dr, Dc, bp, L);
+        create_device();
+    }
+
+    void create_device() {
         int ndev = 0;
         cuda_ok(cudaGetDeviceCount(&ndev), "cudaGetDeviceCount");
         if (ndev == 0) fail(B2_ERR_NO_DEVICE, "no CUDA device");
@@ -251,7 +270,21 @@ struct EngineImpl {
         cuda_ok(cudaMemsetAsync(bar, 0, sizeof(unsigned), st), "memset");
         cuda_ok(cudaMemsetAsync(abort_flag, 0, sizeof(int), st), "memset");
         if (ctas == 1 && !P.debug_delay_ns) {
-            dev::k_pdlp_cta<T, V><<<1, dev::kBlock, 0, st>>>(P, ga);
+            // x' and y' in shared memory when they fit next to the static part
+            dev::GridArgs g1 = ga;
+            const size_t want = ((size_t)L.m + (size_t)L.n) * sizeof(T);
+            cudaFuncAttributes fa{};
+            cuda_ok(cudaFuncGetAttributes(&fa, dev::k_pdlp_cta<T, V>), "attr");
+            int optin = 0;
+            cuda_ok(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, device), "attr");
+            g1.svec_bytes = 0;
+            if (want > 0 && want + fa.sharedSizeBytes <= (size_t)optin) {
+                g1.svec_bytes = (int)((want + 255) / 256 * 256);
+                if ((size_t)g1.svec_bytes + fa.sharedSizeBytes > (size_t)optin) g1.svec_bytes = (int)want;
+                cuda_ok(cudaFuncSetAttribute(dev::k_pdlp_cta<T, V>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             g1.svec_bytes), "cudaFuncSetAttribute");
+            }
+            dev::k_pdlp_cta<T, V><<<1, dev::kBlock, (size_t)g1.svec_bytes, st>>>(P, g1);
             cuda_ok(cudaGetLastError(), "k_pdlp_cta");
             return;
         }
@@ -342,6 +375,80 @@ struct EngineImpl {
         }
     }
 
+    // ---- time-sliced solve (the served stream's whole-GPU lane) ----
+    // begin_slices uploads the initial control state; each slice runs the
+    // current phase for about slice_ms of device time and returns true when
+    // the solve has ended; finish_slices copies the answer out. The FP32 ->
+    // FP64 hand-over happens between slices, as solve() does it in one call.
+    dev::Ctl sl_ctl{};
+    int sl_ctas = 0;
+    double sl_ms = 0.0;
+
+    void begin_slices(const b2_solve_opts& o) {
+        if (o.max_iterations < 0) fail(B2_ERR_INVALID, "max_iterations < 0");
+        dev::Ctl& h = sl_ctl;
+        std::memset(&h, 0, sizeof(h));
+        h.eta = L.eta0;
+        h.omega = L.omega0;
+        h.merit_last_restart = h.merit_prev_cand = h.best_merit = std::numeric_limits<double>::infinity();
+        h.xi = 0; h.yi = 0; h.ax_cur = 0; h.ax_nxt = 1; h.ax_avg = 2; h.aty_cur = 0; h.aty_avg = 1;
+        h.mode = dev::MODE_START;
+        h.phase64 = o.precision == B2_PREC_MIXED ? 0 : 1;
+        *h_stop = 0;
+        cuda_ok(cudaMemcpy(ctl, &h, sizeof(h), cudaMemcpyHostToDevice), "ctl upload");
+        sl_ctas = pick_ctas(o);
+        sl_ms = 0.0;
+    }
+
+    bool slice(const b2_solve_opts& o, double slice_ms, cudaStream_t st) {
+        dev::GridArgs ga = grid_args(o);
+        ga.yield_ns = (unsigned long long)(std::max(0.01, slice_ms) * 1e6);
+        cuda_ok(cudaEventRecord(ev0, st), "event");
+        if (!sl_ctl.phase64) {
+            auto P = params<float>(o, itf);
+            launch<float, float>(P, ga, sl_ctas, st);
+        } else {
+            auto Q = params<double>(o, itd);
+            if (L.exact32) launch<double, float>(Q, ga, sl_ctas, st);
+            else launch<double, double>(Q, ga, sl_ctas, st);
+        }
+        cuda_ok(cudaEventRecord(ev1, st), "event");
+        cuda_ok(cudaEventSynchronize(ev1), "slice");
+        float ms = 0.0f;
+        cuda_ok(cudaEventElapsedTime(&ms, ev0, ev1), "elapsed");
+        sl_ms += ms;
+        check_abort();
+        cuda_ok(cudaMemcpy(&sl_ctl, ctl, sizeof(sl_ctl), cudaMemcpyDeviceToHost), "ctl download");
+        if (sl_ctl.exit_reason != 0) return true;
+        // a hand-over keeps the mode the phase started in (MODE_CONTINUE after
+        // an earlier yield), so it is tested first
+        if (sl_ctl.switch_req) {
+            sl_ctl.mode = dev::MODE_RESUME;
+            sl_ctl.switch_req = 0;
+            sl_ctl.best_merit = std::numeric_limits<double>::infinity();
+            sl_ctl.best_valid = 0;
+            sl_ctl.stall = 0;
+            sl_ctl.phase64 = 1;
+            cuda_ok(cudaMemcpy(ctl, &sl_ctl, sizeof(sl_ctl), cudaMemcpyHostToDevice), "ctl upload");
+            return false;
+        }
+        if (sl_ctl.mode == dev::MODE_CONTINUE) return false;  // yielded
+        return true;
+    }
+
+    void finish_slices(double* x_out, double* y_out, b2_result* res) {
+        last_checks = sl_ctl.checks;
+        if (x_out && L.n) cuda_ok(cudaMemcpy(x_out, out_x, sizeof(double) * L.n, cudaMemcpyDeviceToHost), "x download");
+        if (y_out && L.m) cuda_ok(cudaMemcpy(y_out, out_y, sizeof(double) * L.m, cudaMemcpyDeviceToHost), "y download");
+        if (res) {
+            fill_result(sl_ctl, *res);
+            res->device_ms = sl_ms;
+            res->objective = L.obj_offset;
+            if (x_out)
+                for (int32_t j = 0; j < L.n; ++j) res->objective += L.c[L.inv_c[j]] * x_out[j];
+        }
+    }
+
     // Waits for the persistent kernel while mirroring the caller's stop flag
     // into the mapped word the device polls.
     void wait(const volatile int32_t* stop_flag) {
@@ -419,7 +526,21 @@ EngineImpl* engine_create(const b2_lp_view& U, const b2_lp_view& S, const double
     return e.release();
 }
 
+EngineImpl* engine_create_from_layout(Layout&& L) {
+    std::unique_ptr<EngineImpl> e(new EngineImpl());
+    e->L = std::move(L);
+    e->create_device();
+    return e.release();
+}
+
 void engine_destroy(EngineImpl* e) { delete e; }
+
+size_t engine_bytes(EngineImpl* e) { return e->bytes; }
+void engine_begin_slices(EngineImpl* e, const b2_solve_opts& o) { e->begin_slices(o); }
+bool engine_slice(EngineImpl* e, const b2_solve_opts& o, double slice_ms, void* stream) {
+    return e->slice(o, slice_ms, stream ? (cudaStream_t)stream : e->stream);
+}
+void engine_finish_slices(EngineImpl* e, double* x, double* y, b2_result* r) { e->finish_slices(x, y, r); }
 
 void engine_solve(EngineImpl* e, const b2_solve_opts& o, const volatile int32_t* stop, double* x, double* y,
                   b2_result* r) {

@@ -59,26 +59,85 @@ int pick_lanes(int64_t len, int lane_target) {
     return g;
 }
 
+// Memory cost of one slice: the 32-byte sectors of x (4-byte values) its
+// gathers touch, step by step, plus the col/val stream (32 lanes x 8 bytes =
+// 8 sectors per step, padding included). Rows perm[i .. i+nr), g lanes per row.
+double slice_cost(const std::vector<int64_t>& ptr, const std::vector<int32_t>& idx, const std::vector<int32_t>& perm,
+                  const std::vector<int32_t>& inv_col, int32_t i, int32_t nr, int g, int64_t len) {
+    double sectors = 8.0 * (double)len;
+    uint32_t ids[32];
+    for (int64_t k = 0; k < len; ++k) {
+        int cnt = 0;
+        for (int lane = 0; lane < 32; ++lane) {
+            const int32_t rl = lane / g, sub = lane % g;
+            if (rl >= nr) break;
+            const int32_t r = perm[i + rl];
+            const int64_t b = ptr[r], e = ptr[r + 1];
+            if (e == b) continue;
+            // a padding entry gathers the lane's last real column again
+            int64_t p = b + sub + k * g;
+            if (p >= e) p = b + sub + ((e - 1 - b - sub) / g) * g;
+            if (p < b || p >= e) p = b;
+            ids[cnt++] = (uint32_t)inv_col[idx[p]] >> 3;
+        }
+        std::sort(ids, ids + cnt);
+        sectors += (double)(std::unique(ids, ids + cnt) - ids);
+    }
+    return sectors;
+}
+
 // Builds the sliced format of the rows `perm` (device order) of a CSR whose
 // column indices are mapped through `inv_col`.
 void build_sell(const std::vector<int64_t>& ptr, const std::vector<int32_t>& idx, const std::vector<double>& val,
                 const std::vector<int32_t>& perm, const std::vector<int32_t>& inv_col, int n_cols, int lane_target,
-                bool keep64, SellHost& S) {
+                bool keep64, const BuildParams& bp, SellHost& S) {
     const int32_t rows = (int32_t)perm.size();
     S.n_rows = rows;
     S.n_cols = n_cols;
     S.slice.clear();
+    S.seg.clear();
+    S.seg_slots = 0;
     // pass 1: slice shapes
     struct Shape { int32_t row0, nrows, lg; int64_t len, blk; };
     std::vector<Shape> shapes;
     int64_t blk = 0;
-    for (int32_t i = 0; i < rows;) {
-        const int32_t r0 = perm[i];
-        const int g = pick_lanes(ptr[r0 + 1] - ptr[r0], lane_target);
-        const int32_t nr = std::min<int32_t>(32 / g, rows - i);
+    auto shape_of = [&](int32_t i, int g, int32_t& nr, int64_t& len) {
+        nr = std::min<int32_t>(32 / g, rows - i);
         int64_t lmax = 0;
         for (int32_t t = 0; t < nr; ++t) lmax = std::max<int64_t>(lmax, ptr[perm[i + t] + 1] - ptr[perm[i + t]]);
-        const int64_t len = (lmax + g - 1) / g;
+        len = (lmax + g - 1) / g;
+    };
+    for (int32_t i = 0; i < rows;) {
+        const int32_t r0 = perm[i];
+        const int64_t rlen = ptr[r0 + 1] - ptr[r0];
+        int g = pick_lanes(rlen, lane_target);
+        int32_t nr = 0;
+        int64_t len = 0;
+        shape_of(i, g, nr, len);
+        if (bp.split && rlen >= bp.tune_len) {
+            // long rows: the lanes-per-row whose slice touches the fewest
+            // sectors per entry wins if it beats the length rule by 20%
+            auto entries = [&](int32_t a, int32_t cnt) {
+                int64_t e = 0;
+                for (int32_t t = 0; t < cnt; ++t) e += ptr[perm[a + t] + 1] - ptr[perm[a + t]];
+                return (double)std::max<int64_t>(e, 1);
+            };
+            const double base = slice_cost(ptr, idx, perm, inv_col, i, nr, g, len) / entries(i, nr);
+            double best = base * 0.8;
+            int best_g = g;
+            for (int cg = 1; cg <= 32; cg <<= 1) {
+                if (cg == g) continue;
+                int32_t cnr = 0;
+                int64_t clen = 0;
+                shape_of(i, cg, cnr, clen);
+                const double c = slice_cost(ptr, idx, perm, inv_col, i, cnr, cg, clen) / entries(i, cnr);
+                if (c < best) { best = c; best_g = cg; }
+            }
+            if (best_g != g) {
+                g = best_g;
+                shape_of(i, g, nr, len);
+            }
+        }
         if (len > (int64_t)kLenMask) fail(B2_ERR_UNSUPPORTED, "row too long for the sliced format");
         int lg = 0;
         while ((1 << lg) < g) ++lg;
@@ -92,15 +151,35 @@ void build_sell(const std::vector<int64_t>& ptr, const std::vector<int32_t>& idx
     S.val32.assign((size_t)S.padded, 0.0f);
     if (keep64) S.val64.assign((size_t)S.padded, 0.0);
     else S.val64.clear();
-    S.slice.resize(shapes.size() * 4);
-    // pass 2: fill
+    // pass 2: fill; a slice longer than split_steps becomes segments of at
+    // most that many steps (at most 255 of them), consecutive slice records
+    // over the same rows and storage
+    const int64_t split_at = bp.split ? std::max(1, bp.split_steps) : INT64_MAX;
+    S.slice.reserve(shapes.size() * 4);
     for (size_t s = 0; s < shapes.size(); ++s) {
         const Shape& sh = shapes[s];
         const int g = 1 << sh.lg;
-        S.slice[4 * s + 0] = sh.row0;
-        S.slice[4 * s + 1] = (int32_t)((uint32_t)sh.len | ((uint32_t)sh.lg << kLenBits));
-        S.slice[4 * s + 2] = (int32_t)(uint32_t)sh.blk;
-        S.slice[4 * s + 3] = 0;
+        if (sh.len > split_at) {
+            const int64_t seg_steps = std::max<int64_t>(split_at, (sh.len + 254) / 255);
+            const int64_t q_count = (sh.len + seg_steps - 1) / seg_steps;
+            const int64_t group = S.n_groups();
+            if (group + 1 >= (1 << 24)) fail(B2_ERR_UNSUPPORTED, "too many split slices");
+            S.seg.push_back((int32_t)q_count);
+            S.seg.push_back((int32_t)S.seg_slots);
+            S.seg_slots += q_count;
+            for (int64_t q = 0; q < q_count; ++q) {
+                const int64_t l0 = q * seg_steps, l1 = std::min(sh.len, l0 + seg_steps);
+                S.slice.push_back(sh.row0);
+                S.slice.push_back((int32_t)((uint32_t)(l1 - l0) | ((uint32_t)sh.lg << kLenBits)));
+                S.slice.push_back((int32_t)(uint32_t)(sh.blk + l0));
+                S.slice.push_back((int32_t)((uint32_t)(group + 1) | ((uint32_t)q << 24)));
+            }
+        } else {
+            S.slice.push_back(sh.row0);
+            S.slice.push_back((int32_t)((uint32_t)sh.len | ((uint32_t)sh.lg << kLenBits)));
+            S.slice.push_back((int32_t)(uint32_t)sh.blk);
+            S.slice.push_back(0);
+        }
         for (int lane = 0; lane < 32; ++lane) {
             const int32_t rl = lane / g, sub = lane % g;
             uint32_t last_col = 0;
@@ -184,8 +263,8 @@ void build_layout(const b2_lp_view& U, const b2_lp_view& S, const double* Dr, co
     for (int32_t i = 0; i < m; ++i) L.inv_r[L.perm_r[i]] = i;
     for (int32_t j = 0; j < n; ++j) L.inv_c[L.perm_c[j]] = j;
 
-    build_sell(aptr, aidx, aval, L.perm_r, L.inv_c, n, target, !L.exact32, L.A);
-    build_sell(tptr, tidx, tval, L.perm_c, L.inv_r, m, target, !L.exact32, L.AT);
+    build_sell(aptr, aidx, aval, L.perm_r, L.inv_c, n, target, !L.exact32, bp, L.A);
+    build_sell(tptr, tidx, tval, L.perm_c, L.inv_r, m, target, !L.exact32, bp, L.AT);
 
     L.b.resize(m); L.rU.resize(m); L.dr2.resize(m);
     for (int32_t i = 0; i < m; ++i) {

@@ -32,7 +32,12 @@ struct SellHost {
     std::vector<float> val32;
     std::vector<double> val64;        // only when values are not exact in FP32
     int64_t padded = 0;               // stored entries including padding
+    // split slices: per group {segments, first segment slot}; slice.w of a
+    // segment = group + 1 | segment << 24 (0: unsplit)
+    std::vector<int32_t> seg;
+    int64_t seg_slots = 0;            // segments in all groups (32 partial sums each)
     int64_t n_slices() const { return (int64_t)slice.size() / 4; }
+    int64_t n_groups() const { return (int64_t)seg.size() / 2; }
 };
 
 constexpr int kLenBits = 27;
@@ -60,6 +65,13 @@ struct Layout {
 struct BuildParams {
     int lane_target = 16;   // entries per lane that decides lanes-per-row
     int sigma_window = 1024;
+    // whole-GPU engine: rows of at least `tune_len` entries get the
+    // lanes-per-row that touches the fewest memory sectors (cost model over
+    // their actual column indices), and slices longer than `split_steps`
+    // steps are split into segments that run on different warps
+    bool split = false;
+    int tune_len = 256;
+    int split_steps = 32;
 };
 
 // Validates the PDLP form and builds the device layout. Throws Error.
@@ -85,6 +97,14 @@ void engine_info(EngineImpl* e, b2_engine_info* info);
 void engine_spmv(EngineImpl* e, int which, const double* x, double* y);
 int engine_trace(EngineImpl* e, double* out, int max_records);
 void engine_spmv_bench(EngineImpl* e, int which, int precision, int reps, void* stream, double* avg_ms);
+// An engine over a layout built beforehand (build_layout), and the
+// time-sliced form of engine_solve used by the served stream: begin, slices of
+// about slice_ms of device time (true when the solve has ended), finish.
+EngineImpl* engine_create_from_layout(Layout&& L);
+size_t engine_bytes(EngineImpl* e);
+void engine_begin_slices(EngineImpl* e, const b2_solve_opts& o);
+bool engine_slice(EngineImpl* e, const b2_solve_opts& o, double slice_ms, void* stream);
+void engine_finish_slices(EngineImpl* e, double* x, double* y, b2_result* r);
 
 // The allocation-free one-CTA solve (noalloc.cu). Throws Error.
 void solve_noalloc(const b2_lp_view& U, const b2_lp_view& S, const double* Dr, const double* Dc,
@@ -99,5 +119,14 @@ void batch_solve(BatchImpl* b, const b2_solve_opts& o, const volatile int32_t* s
 void batch_solution(BatchImpl* b, int i, double* x, double* y);
 void batch_info(BatchImpl* b, b2_batch_info* inf);
 void batch_spmv(BatchImpl* b, int i, int which, const double* x, double* y);
+
+// The served stream (serve.cu). All functions throw Error.
+struct ServerImpl;
+ServerImpl* server_create(const b2_server_opts& so, const b2_solve_opts& o);
+void server_destroy(ServerImpl* s);
+int64_t server_submit(ServerImpl* s, const b2_lp_view& U);
+int server_wait(ServerImpl* s, int64_t ticket, double timeout_s, double* x, double* y, b2_result* res,
+                b2_request_info* info);
+void server_stats(ServerImpl* s, b2_server_stats* out);
 
 }  // namespace b2

@@ -1,0 +1,140 @@
+"""The served stream (b2_server_*): LPs arriving over time, continuous batching.
+
+* every answer is certified by the oracle's restated verify() and agrees with
+  the reference's dual simplex (golden fixtures);
+* rounds pause LPs at their deadline and resume them in the next round; the
+  answer is bit-identical to the uninterrupted batched solve of the same LP;
+* an LP's answer is bit-identical alone and in a mix that arrives around it;
+* the whole-GPU lane (time-sliced one-LP engine) returns the one-LP engine's
+  answer bit for bit;
+* admission keeps the resident footprint under the HBM budget; a malformed
+  request fails alone and the server keeps serving.
+"""
+import time
+
+import numpy as np
+import pytest
+
+import b200pdlp as B
+import oracle as O
+from conftest import as_form, fixture_names, golden_index, load_fixture, random_case, rel
+
+pytestmark = pytest.mark.gpu
+
+G = golden_index()
+TOL = 1e-6
+
+
+def fixture_problems():
+    names = fixture_names()
+    return names, [load_fixture(n) for n in names]
+
+
+def certified(U, res, ref_obj):
+    v = O.verify(as_form(U), res.x, res.y)
+    assert max(v["eps_P"], v["eps_D"], v["eps_G"]) <= TOL * (1 + 1e-9), v
+    assert rel(v["objective"], ref_obj) <= 1e-5
+    return v
+
+
+@pytest.mark.parametrize("precision", [B.PREC_MIXED, B.PREC_FP64])
+def test_served_answers_certified_and_equal_to_uninterrupted_batch(precision):
+    names, probs = fixture_problems()
+    keys = sorted(G["random"].keys())
+    refs = [G["fixtures"][n]["simplex"]["objective"] for n in names]
+    for k in keys:
+        _, U, S, Dr, Dc, g = random_case(k)
+        probs.append((U, S, Dr, Dc))
+        refs.append(g["simplex"]["objective"])
+    # tiny rounds: every LP is paused and resumed many times
+    with B.Server(round_ms=0.2, precision=precision, max_iterations=500000, tol=TOL) as srv:
+        tickets = [srv.submit(U) for (U, _, _, _) in probs]
+        out = [srv.wait(t, timeout_s=300.0) for t in tickets]
+    assert all(o is not None for o in out)
+    assert max(info["rounds"] for _, info in out) > 3
+    with B.Batch(probs) as bt:
+        res, _ = bt.solve(max_iterations=500000, tol=TOL, precision=precision)
+        for i, (U, S, Dr, Dc) in enumerate(probs):
+            r, info = out[i]
+            assert r.converged, (i, r.stats)
+            assert info["lane"] == 0
+            certified(U, r, refs[i])
+            x, y = bt.solution(i)
+            assert r.iterations == res[i]["iterations"]
+            np.testing.assert_array_equal(r.x, x)
+            np.testing.assert_array_equal(r.y, y)
+
+
+def test_answer_is_identical_alone_and_in_an_arriving_mix():
+    names, probs = fixture_problems()
+    target = names.index("israel")
+    U = probs[target][0]
+    with B.Server(round_ms=0.5) as srv:
+        alone, _ = srv.wait(srv.submit(U), timeout_s=300.0)
+    shapes = B.batch_family_shapes(40, seed=11, m_lo=50, m_hi=800)
+    others = []
+    for (m, n, k, seed) in shapes:
+        lp = B.gen_random_lp(m, n, k, seed, True)
+        others.append(B.prepare(lp)[0])
+    with B.Server(round_ms=0.5) as srv:
+        early = [srv.submit(o) for o in others[:20]]
+        time.sleep(0.01)
+        t = srv.submit(U)
+        time.sleep(0.005)
+        late = [srv.submit(o) for o in others[20:]]
+        mixed, info = srv.wait(t, timeout_s=300.0)
+        rest = [srv.wait(k, timeout_s=300.0) for k in early + late]
+        st = srv.stats()
+    assert all(r is not None and r[0].converged for r in rest)
+    assert st["completed"] == 41 and st["failed"] == 0 and st["rounds"] >= 1
+    assert alone.iterations == mixed.iterations
+    np.testing.assert_array_equal(alone.x, mixed.x)
+    np.testing.assert_array_equal(alone.y, mixed.y)
+    certified(U, mixed, G["fixtures"]["israel"]["simplex"]["objective"])
+
+
+@pytest.mark.parametrize("precision", [B.PREC_MIXED, B.PREC_FP64])
+def test_whole_gpu_lane_matches_one_lp_engine(precision):
+    _, U, S, Dr, Dc, g = random_case(sorted(G["random"].keys())[0])
+    with B.Engine(U, S, Dr, Dc) as eng:
+        ref = eng.solve(max_iterations=500000, tol=TOL, precision=precision)
+    with B.Server(grid_nnz=1, grid_slice_ms=0.3, precision=precision, max_iterations=500000, tol=TOL) as srv:
+        r, info = srv.wait(srv.submit(U), timeout_s=300.0)
+        st = srv.stats()
+    assert info["lane"] == 1 and info["rounds"] > 1 and st["grid_slices"] == info["rounds"]
+    assert r.converged and r.iterations == ref.iterations
+    np.testing.assert_array_equal(r.x, ref.x)
+    np.testing.assert_array_equal(r.y, ref.y)
+    certified(U, r, g["simplex"]["objective"])
+
+
+def test_admission_keeps_footprint_under_budget():
+    shapes = B.batch_family_shapes(24, seed=3, m_lo=200, m_hi=600)
+    lps = [B.prepare(B.gen_random_lp(m, n, k, seed, True))[0] for (m, n, k, seed) in shapes]
+    budget = 3_000_000  # a few LPs at a time
+    with B.Server(hbm_budget_bytes=budget, round_ms=1.0) as srv:
+        ts = [srv.submit(U) for U in lps]
+        out = [srv.wait(t, timeout_s=300.0) for t in ts]
+        st = srv.stats()
+    assert all(r is not None and r[0].converged for r in out)
+    sizes = [info["device_bytes"] for _, info in out]
+    assert max(sizes) <= budget
+    assert st["peak_bytes"] <= budget
+    assert st["bytes_in_use"] == 0 and st["resident"] == 0
+
+
+def test_malformed_request_fails_alone():
+    U, S, Dr, Dc = load_fixture("afiro")
+    bad = B.RangedLP.like(U)
+    bad.col = bad.col.copy()
+    bad.col[0] = U.n + 7
+    with B.Server(round_ms=1.0) as srv:
+        t_bad = srv.submit(bad)
+        t_ok = srv.submit(U)
+        with pytest.raises(B.B2Error) as e:
+            srv.wait(t_bad, timeout_s=60.0)
+        assert e.value.code == B.B2_ERR_INVALID
+        r, _ = srv.wait(t_ok, timeout_s=60.0)
+        st = srv.stats()
+    assert r.converged and st["failed"] == 1 and st["completed"] == 1
+    certified(U, r, G["fixtures"]["afiro"]["simplex"]["objective"])

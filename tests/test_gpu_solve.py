@@ -172,3 +172,27 @@ def test_inequality_rows_and_free_columns():
         assert worst <= 1e-7 * (1 + 1e-6)
         vr = O.verify(as_form(U), ref["x"], ref["y"])
         assert rel(v["objective"], vr["objective"]) <= 1e-5
+
+
+def test_transport_split_layout_solve_certified():
+    """A transportation LP on the whole-GPU layout (tuned, split slices) and on
+    the batched layout (neither): both certified, objectives agree."""
+    lp = B.gen_transport(300, 500, 7)
+    U, S, Dr, Dc, _ = B.prepare(lp)
+    r = B.solve_pdhg_gpu(U, S, Dr, Dc, 0.99, 500000, 64, 1e-6)
+    assert r.converged
+    v = O.verify(as_form(U), r.x, r.y)
+    assert max(v["eps_P"], v["eps_D"], v["eps_G"]) <= 1e-6 * (1 + 1e-9)
+    with B.Batch([(U, S, Dr, Dc)]) as bt:
+        res, _ = bt.solve(max_iterations=500000, tol=1e-6)
+        x, y = bt.solution(0)
+    assert res[0]["converged"]
+    v2 = O.verify(as_form(U), x, y)
+    assert max(v2["eps_P"], v2["eps_D"], v2["eps_G"]) <= 1e-6 * (1 + 1e-9)
+    assert rel(v["objective"], v2["objective"]) <= 1e-5
+    # repeated solves on the split layout are bit-identical (fixed segment order)
+    with B.Engine(U, S, Dr, Dc) as eng:
+        a = eng.solve(max_iterations=3000, tol=1e-9)
+        b = eng.solve(max_iterations=3000, tol=1e-9)
+    np.testing.assert_array_equal(a.x, b.x)
+    np.testing.assert_array_equal(a.y, b.y)

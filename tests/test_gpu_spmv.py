@@ -62,3 +62,13 @@ def test_spmv_empty_rows_and_columns():
     lp = B.RangedLP(m, n, row, col, val, c, rL, rU, np.zeros(n), np.full(n, 10.0))
     s, Dr, Dc = B.scale(lp)
     _check_engine(lp, s, Dr, Dc)
+
+
+@pytest.mark.parametrize("shape", [(300, 700), (700, 300)])
+def test_spmv_transport_tuned_and_split_slices(shape):
+    """Long rows on the whole-GPU layout: lanes-per-row chosen by the sector
+    cost model, slices longer than 32 steps split over several warps whose
+    partial sums one warp adds in segment order."""
+    lp = B.gen_transport(shape[0], shape[1], 3)
+    U, S, Dr, Dc, _ = B.prepare(lp)
+    _check_engine(U, S, Dr, Dc, seed=2)

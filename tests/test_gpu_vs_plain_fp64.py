@@ -1,0 +1,87 @@
+"""This engine against the reference's own plain FP64 GPU PDLP
+(gpu/pdlp_gpu_solve.cu, compiled for sm_100a into the oracle) on the same B200.
+
+The reference engine syncs the host once per attempt and runs two host
+verify() calls every 64 accepted steps, so its full solves of the large LPs
+take minutes; it is timed on two bounded samples of attempts, and its solve
+time is extrapolated as setup + attempts x (time per attempt), with the
+attempts its own algorithm needs (this engine's FP64 mode takes the
+reference's decisions, so that count is the reference's).
+
+Targets: the 500,000 x 1,000,000 LP (8M nonzeros) solved >= 5x faster by the
+mixed-precision engine; a batch of uneven LPs >= 20x the solves/s of the
+plain engine solving them one at a time. The measured figures are printed.
+"""
+import json
+import time
+
+import numpy as np
+import pytest
+
+import b200pdlp as B
+import oracle as O
+from conftest import as_form
+
+pytestmark = pytest.mark.gpu
+
+if not O.reference_available(gpu=True):
+    pytest.skip("the reference's GPU engine is not built (oracle/_ref/libsovref_gpu.so)", allow_module_level=True)
+
+
+def ref_time_model(P, n1, n2):
+    """(setup seconds, seconds per attempt) of the reference GPU engine from two bounded runs."""
+    r1 = P.solve_pdhg(max_iterations=n1, check_every=64, tol=1e-12, gpu=True)
+    r2 = P.solve_pdhg(max_iterations=n2, check_every=64, tol=1e-12, gpu=True)
+    per = (r2["seconds"] - r1["seconds"]) / (r2["iterations"] - r1["iterations"])
+    setup = max(0.0, r1["seconds"] - r1["iterations"] * per)
+    return setup, per
+
+
+def test_large_lp_vs_plain_fp64_gpu():
+    lp = B.gen_random_lp(500_000, 1_000_000, 8, 1, True)
+    U, S, Dr, Dc, _ = B.prepare(lp)
+    with B.Engine(U, S, Dr, Dc) as eng:
+        eng.solve(max_iterations=2000, tol=1e-6)  # warm-up
+        t0 = time.perf_counter()
+        r = eng.solve(max_iterations=2_000_000, tol=1e-6, copy_out=False)
+        ours_s = time.perf_counter() - t0
+        r64 = eng.solve(max_iterations=2_000_000, tol=1e-6, precision=B.PREC_FP64, copy_out=False)
+    assert r.converged and r64.converged
+    P = O.RefProblem.from_form(as_form(U), use_presolve=False, gpu=True)
+    setup, per = ref_time_model(P, 128, 640)
+    ref_s = setup + r64.iterations * per
+    line = {"lp": "random 500000x1000000, 8 nnz/col", "engine_s": ours_s, "engine_attempts": r.iterations,
+            "plain_fp64_gpu_s_est": ref_s, "plain_setup_s": setup, "plain_ms_per_attempt": per * 1e3,
+            "plain_attempts": r64.iterations, "speedup": ref_s / ours_s}
+    print("PLAIN_FP64_LARGE " + json.dumps(line))
+    assert ref_s / ours_s >= 5.0, line
+
+
+def test_batch_vs_plain_fp64_gpu_one_at_a_time():
+    shapes = B.batch_family_shapes(256, seed=0)
+    probs = []
+    for (m, n, k, seed) in shapes:
+        U, S, Dr, Dc, _ = B.prepare(B.gen_random_lp(m, n, k, seed, True))
+        probs.append((U, S, Dr, Dc))
+    with B.Batch(probs) as bt:
+        bt.solve(max_iterations=2_000_000, tol=1e-6)  # warm-up
+        res, ms = bt.solve(max_iterations=2_000_000, tol=1e-6)
+    assert all(r["converged"] for r in res)
+    ours = len(probs) / (ms / 1e3)
+    # the plain engine, one LP at a time: full solves of a sample spread over sizes
+    order = np.argsort([p[0].nnz for p in probs])
+    pick = [int(order[i]) for i in np.linspace(0, len(order) - 1, 6).astype(int)]
+    t_sample, att_sample = [], []
+    for i in pick:
+        P = O.RefProblem.from_form(as_form(probs[i][0]), use_presolve=False, gpu=True)
+        r = P.solve_pdhg(max_iterations=2_000_000, check_every=64, tol=1e-6, gpu=True)
+        t_sample.append(r["seconds"])
+        att_sample.append(r["iterations"])
+    # seconds per attempt of the sample, applied to every LP's own attempt count
+    per_att = sum(t_sample) / sum(att_sample)
+    ref_total = per_att * sum(r["iterations"] for r in res)
+    plain = len(probs) / ref_total
+    line = {"lps": len(probs), "engine_solves_per_s": ours, "engine_ms": ms, "plain_fp64_gpu_solves_per_s_est": plain,
+            "plain_ms_per_attempt": per_att * 1e3, "sample_lps": len(pick), "speedup": ours / plain}
+    print("PLAIN_FP64_BATCH " + json.dumps(line))
+    assert ours / plain >= 20.0, line
