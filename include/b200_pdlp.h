@@ -240,6 +240,8 @@ typedef struct b2_server_opts {
     double grid_slice_ms;     /* device time of one whole-GPU slice; <= 0: 20 ms        */
     int64_t cluster_nnz;      /* stored entries (A and A^T) from which a batched LP is solved by
                                  a cluster of 8 CTAs; 0: 300,000; < 0: never             */
+    int64_t gpu_scale_nnz;    /* nonzeros from which an LP is scaled on the GPU (b2_scale_gpu,
+                                 the same bits); 0: 1,000,000; < 0: never                */
 } b2_server_opts;
 
 typedef struct b2_request_info {
@@ -281,6 +283,13 @@ void b2_server_destroy(b2_server* s);
  * COO order (nnz), c/l/u (n), rL/rU (m), Dr (m), Dc (n). */
 int b2_scale(const b2_lp_view* lp, int32_t ruiz_passes, double* val_s, double* c_s, double* rL_s, double* rU_s,
              double* l_s, double* u_s, double* Dr, double* Dc);
+
+/* The same scaling computed on the current GPU, bit for bit equal to b2_scale
+ * (and so to the reference's scale()): maxima and products are exact, and the
+ * Pock-Chambolle row / column sums add entries in COO order as the host loop
+ * does. For ingest of large LPs, whose host scaling takes seconds. */
+int b2_scale_gpu(const b2_lp_view* lp, int32_t ruiz_passes, double* val_s, double* c_s, double* rL_s,
+                 double* rU_s, double* l_s, double* u_s, double* Dr, double* Dc);
 
 /* Synthetic LPs of the benchmark shapes (seeded, deterministic):
  * equality-form LP min c'x, Ax = b, 0 <= x <= 10, `k` distinct uniform rows per

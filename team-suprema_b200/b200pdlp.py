@@ -43,7 +43,7 @@ EXPORTED = [
     "b2_batch_create", "b2_batch_solve", "b2_batch_get_solution", "b2_batch_get_info", "b2_batch_spmv",
     "b2_batch_destroy",
     "b2_server_create", "b2_server_submit", "b2_server_wait", "b2_server_stats_get", "b2_server_destroy",
-    "b2_scale",
+    "b2_scale", "b2_scale_gpu",
     "b2_gen_random_lp", "b2_gen_transport", "b2_last_error", "b2_version",
 ]
 
@@ -89,7 +89,7 @@ class BatchInfo(C.Structure):
 class ServerOpts(C.Structure):
     _fields_ = [("hbm_budget_bytes", C.c_double), ("round_ms", C.c_double), ("max_resident", C.c_int32),
                 ("prep_threads", C.c_int32), ("grid_nnz", C.c_int64), ("grid_slice_ms", C.c_double),
-                ("cluster_nnz", C.c_int64)]
+                ("cluster_nnz", C.c_int64), ("gpu_scale_nnz", C.c_int64)]
 
 
 class RequestInfo(C.Structure):
@@ -157,6 +157,7 @@ def lib():
             L.b2_server_destroy.argtypes = [vp]
             L.b2_server_destroy.restype = None
             L.b2_scale.argtypes = [C.POINTER(_LPView), i32] + [vp] * 8
+            L.b2_scale_gpu.argtypes = [C.POINTER(_LPView), i32] + [vp] * 8
             L.b2_gen_random_lp.argtypes = [i32, i32, i32, C.c_uint64, i32] + [vp] * 8
             L.b2_gen_transport.argtypes = [i32, i32, C.c_uint64] + [vp] * 8
             _lib = L
@@ -465,9 +466,9 @@ class Server:
 
     def __init__(self, hbm_budget_bytes: float = 0.0, round_ms: float = 0.0, max_resident: int = 0,
                  prep_threads: int = 0, grid_nnz: int = 0, grid_slice_ms: float = 0.0, cluster_nnz: int = 0,
-                 **opts):
+                 gpu_scale_nnz: int = 0, **opts):
         so = ServerOpts(float(hbm_budget_bytes), float(round_ms), int(max_resident), int(prep_threads),
-                        int(grid_nnz), float(grid_slice_ms), int(cluster_nnz))
+                        int(grid_nnz), float(grid_slice_ms), int(cluster_nnz), int(gpu_scale_nnz))
         o = default_opts(**opts)
         h = C.c_void_p()
         _check(lib().b2_server_create(C.byref(so), C.byref(o), C.byref(h)))
@@ -520,14 +521,16 @@ class Server:
 
 
 # ------------------------------------------------------------- host-side prep
-def scale(lp: RangedLP, ruiz_passes: int = 10):
-    """Ruiz + Pock-Chambolle scaling (src/scaling.cpp:25-84). Returns (scaled, Dr, Dc)."""
+def scale(lp: RangedLP, ruiz_passes: int = 10, on_gpu: bool = False):
+    """Ruiz + Pock-Chambolle scaling (src/scaling.cpp:25-84). Returns (scaled, Dr, Dc).
+    on_gpu: the same computation on the current GPU (b2_scale_gpu), bit for bit."""
     lp = RangedLP.like(lp)
     vs = np.zeros(max(lp.nnz, 1)); cs = np.zeros(max(lp.n, 1)); rls = np.zeros(max(lp.m, 1))
     rus = np.zeros(max(lp.m, 1)); ls = np.zeros(max(lp.n, 1)); us = np.zeros(max(lp.n, 1))
     Dr = np.zeros(max(lp.m, 1)); Dc = np.zeros(max(lp.n, 1))
     v = lp.view()
-    _check(lib().b2_scale(C.byref(v), ruiz_passes, *[_ptr(a) for a in (vs, cs, rls, rus, ls, us, Dr, Dc)]))
+    fn = lib().b2_scale_gpu if on_gpu else lib().b2_scale
+    _check(fn(C.byref(v), ruiz_passes, *[_ptr(a) for a in (vs, cs, rls, rus, ls, us, Dr, Dc)]))
     s = RangedLP(lp.m, lp.n, lp.row, lp.col, vs[:lp.nnz], cs[:lp.n], rls[:lp.m], rus[:lp.m], ls[:lp.n],
                  us[:lp.n], lp.obj_offset)
     return s, Dr[:lp.m], Dc[:lp.n]

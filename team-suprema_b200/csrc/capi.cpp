@@ -269,6 +269,14 @@ int b2_scale(const b2_lp_view* lp, int32_t ruiz_passes, double* val_s, double* c
     });
 }
 
+int b2_scale_gpu(const b2_lp_view* lp, int32_t ruiz_passes, double* val_s, double* c_s, double* rL_s, double* rU_s,
+             double* l_s, double* u_s, double* Dr, double* Dc) {
+    return b2::guarded([&] {
+        if (!lp) b2::fail(B2_ERR_INVALID, "null argument");
+        b2::scale_lp_gpu(*lp, ruiz_passes, val_s, c_s, rL_s, rU_s, l_s, u_s, Dr, Dc);
+    });
+}
+
 int b2_gen_random_lp(int32_t m, int32_t n, int32_t k, uint64_t seed, int32_t fp32_values, int32_t* row,
                      int32_t* col, double* val, double* c, double* rL, double* rU, double* l, double* u) {
     return b2::guarded([&] { b2::gen_random_lp(m, n, k, seed, fp32_values != 0, row, col, val, c, rL, rU, l, u); });

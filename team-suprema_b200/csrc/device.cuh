@@ -370,15 +370,76 @@ __device__ __forceinline__ AccT slice_dot(const SellDev& S, const V* vbase, int4
     return acc;
 }
 
+// Sum of a lane's partials of a split group in segment order; the loads are
+// issued 16 at a time (the adds stay one chain, so the order is fixed).
+template <class AccT>
+__device__ __forceinline__ AccT sum_partials(const double* part, int segments, int lane) {
+    AccT tot = AccT(0);
+    int t = 0;
+    for (; t + 16 <= segments; t += 16) {
+        double v[16];
+#pragma unroll
+        for (int k = 0; k < 16; ++k) v[k] = __ldcg(part + (t + k) * 32 + lane);
+#pragma unroll
+        for (int k = 0; k < 16; ++k) tot += (AccT)v[k];
+    }
+    for (; t < segments; ++t) tot += (AccT)__ldcg(part + t * 32 + lane);
+    return tot;
+}
+
 // A split slice is one of `segments` consecutive slice records over the same
 // rows, each covering a range of steps (slice.w = group + 1 | segment << 24;
-// 0 for an unsplit slice). Every segment publishes its lanes' partial sums;
-// the warp that completes the group adds them in segment order (the result
-// does not depend on which warp that is) and alone goes on to the row's
-// epilogue. Returns whether this warp holds complete row sums in `acc`.
+// 0 for an unsplit slice); only the whole-GPU layout has them. Every segment
+// publishes its lanes' partial sums and counts itself in; the warp of segment
+// 0 owns the rows: it waits (bounded) until the others have arrived, adds the
+// partials in segment order and alone runs the rows' epilogue, so the sums,
+// and which CTA's reductions the rows land in, never depend on timing.
+// Waits cannot form a cycle: segment 0 waits only on the next segments - 1
+// slice records, and the launch keeps segments <= the group's warp count, so
+// none of them is a later slice of the waiting warp itself.
+// Returns whether this warp holds complete row sums in `acc`.
 template <int GK, class AccT>
-__device__ __forceinline__ bool seg_finish(const SellDev& S, int4 sl, int lane, AccT& acc) {
-    if (GK != GK_GRID || sl.w == 0) return true;  // only the whole-GPU layout splits slices
+__device__ __forceinline__ bool seg_finish(const SellDev& S, int4 sl, int lane, AccT& acc, const Group& g) {
+    if (GK != GK_GRID || sl.w == 0) return true;
+    const int grp = (sl.w & 0xFFFFFF) - 1, q = (int)((unsigned)sl.w >> 24);
+    const int2 info = __ldg(S.seg + grp);
+    double* part = S.seg_part + (size_t)info.y * 32;
+    __stcg(part + q * 32 + lane, (double)acc);
+    __threadfence();
+    __syncwarp();
+    if (q != 0) {
+        if (lane == 0) atomicAdd(S.seg_cnt + grp, 1u);
+        return false;
+    }
+    int ok = 1;
+    if (lane == 0) {
+        const unsigned want = (unsigned)(info.x - 1);
+        const unsigned long long t0 = gtimer();
+        unsigned spins = 0;
+        for (;;) {
+            unsigned cur;
+            asm volatile("ld.acquire.gpu.u32 %0,[%1];" : "=r"(cur) : "l"(S.seg_cnt + grp) : "memory");
+            if (cur == want) break;
+            if ((++spins & 63u) == 0) {
+                if (*(volatile int*)g.abort || gtimer() - t0 > g.timeout_ns) { atomicExch(g.abort, 1); ok = 0; break; }
+            }
+        }
+        if (ok) S.seg_cnt[grp] = 0u;  // all have arrived: ready for the next product
+    }
+    ok = __shfl_sync(0xffffffffu, ok, 0);
+    __syncwarp();
+    if (!ok) return false;  // the group's next barrier reports the abort
+    __threadfence();
+    acc = sum_partials<AccT>(part, info.x, lane);
+    return true;
+}
+
+// The same for a product with no reductions behind it (the standalone SpMV):
+// whichever warp completes the group adds the partials in segment order, so
+// nobody waits and the sums are still the same bits.
+template <class AccT>
+__device__ __forceinline__ bool seg_finish_last(const SellDev& S, int4 sl, int lane, AccT& acc) {
+    if (sl.w == 0) return true;
     const int grp = (sl.w & 0xFFFFFF) - 1, q = (int)((unsigned)sl.w >> 24);
     const int2 info = __ldg(S.seg + grp);
     double* part = S.seg_part + (size_t)info.y * 32;
@@ -388,15 +449,15 @@ __device__ __forceinline__ bool seg_finish(const SellDev& S, int4 sl, int lane, 
     unsigned last = 0;
     if (lane == 0) last = atomicAdd(S.seg_cnt + grp, 1u) == (unsigned)(info.x - 1) ? 1u : 0u;
     last = __shfl_sync(0xffffffffu, last, 0);
+    __syncwarp();
     if (!last) return false;
     __threadfence();
-    AccT tot = AccT(0);
-    for (int t = 0; t < info.x; ++t) tot += (AccT)__ldcg(part + t * 32 + lane);
-    acc = tot;
-    if (lane == 0) S.seg_cnt[grp] = 0u;  // the next product over this matrix comes after a barrier
+    acc = sum_partials<AccT>(part, info.x, lane);
+    if (lane == 0) S.seg_cnt[grp] = 0u;  // the next product comes after this kernel
     return true;
 }
-// A pass that needs no product over a split slice still runs the row's
+
+// A pass that needs no product over a split slice still runs the rows'
 // epilogue once: in the warp of segment 0.
 template <int GK>
 __device__ __forceinline__ bool seg_first(int4 sl) {
@@ -477,7 +538,7 @@ __device__ void pass_rows_step(const KParams<T>& P, const Ctl& c, const Group& g
     for (int s = g.gw; s < P.A.n_slices; s += g.nw) {
         const int4 sl = __ldg(P.A.slice + s);
         T acc = slice_dot<GK, T, V, T>(P.A, vb, sl, lane, xn);
-        if (!seg_finish<GK, T>(P.A, sl, lane, acc)) continue;
+        if (!seg_finish<GK, T>(P.A, sl, lane, acc, g)) continue;
         const int lg = (int)((uint32_t)sl.y >> kLenBits);
         const int row = sl.x + (lane >> lg);
         if ((lane & ((1 << lg) - 1)) == 0 && row < P.m) {
@@ -512,7 +573,7 @@ __device__ void pass_cols_step(const KParams<T>& P, const Ctl& c, const Group& g
         for (int s = g.gw; s < P.AT.n_slices; s += g.nw) {
             const int4 sl = __ldg(P.AT.slice + s);
             T acc = slice_dot<GK, T, V, T>(P.AT, vb, sl, lane, y);
-            if (!seg_finish<GK, T>(P.AT, sl, lane, acc)) continue;
+            if (!seg_finish<GK, T>(P.AT, sl, lane, acc, g)) continue;
             const int lg = (int)((uint32_t)sl.y >> kLenBits);
             const int j = sl.x + (lane >> lg);
             if ((lane & ((1 << lg) - 1)) == 0 && j < P.n) {
@@ -544,7 +605,7 @@ __device__ void pass_rows_check(const KParams<T>& P, const Ctl& c, const Group& 
         double acc = 0.0;
         if (has_avg) {
             acc = slice_dot<GK, double, V, double>(P.A, vb, sl, lane, P.xsum);
-            if (!seg_finish<GK, double>(P.A, sl, lane, acc)) continue;
+            if (!seg_finish<GK, double>(P.A, sl, lane, acc, g)) continue;
         } else if (!seg_first<GK>(sl)) {
             continue;
         }
@@ -581,7 +642,7 @@ __device__ void pass_cols_check(const KParams<T>& P, const Ctl& c, const Group& 
         double acc = 0.0;
         if (has_avg) {
             acc = slice_dot<GK, double, V, double>(P.AT, vb, sl, lane, P.ysum);
-            if (!seg_finish<GK, double>(P.AT, sl, lane, acc)) continue;
+            if (!seg_finish<GK, double>(P.AT, sl, lane, acc, g)) continue;
         } else if (!seg_first<GK>(sl)) {
             continue;
         }
@@ -872,7 +933,7 @@ __device__ bool solve_body(const KParams<T>& P, const Group& g) {
             for (int k = g.gw; k < P.A.n_slices; k += g.nw) {
                 const int4 sl = __ldg(P.A.slice + k);
                 T acc = slice_dot<GK, T, V, T>(P.A, vb, sl, lane, P.it.x[s.xi]);
-                if (!seg_finish<GK, T>(P.A, sl, lane, acc)) continue;
+                if (!seg_finish<GK, T>(P.A, sl, lane, acc, g)) continue;
                 const int lg = (int)((uint32_t)sl.y >> kLenBits);
                 const int i = sl.x + (lane >> lg);
                 if ((lane & ((1 << lg) - 1)) == 0 && i < P.m) ax[i] = acc;
@@ -883,7 +944,7 @@ __device__ bool solve_body(const KParams<T>& P, const Group& g) {
                 for (int k = g.gw; k < P.AT.n_slices; k += g.nw) {
                     const int4 sl = __ldg(P.AT.slice + k);
                     T acc = slice_dot<GK, T, V, T>(P.AT, vt, sl, lane, P.it.y[s.yi]);
-                    if (!seg_finish<GK, T>(P.AT, sl, lane, acc)) continue;
+                    if (!seg_finish<GK, T>(P.AT, sl, lane, acc, g)) continue;
                     const int lg = (int)((uint32_t)sl.y >> kLenBits);
                     const int j = sl.x + (lane >> lg);
                     if ((lane & ((1 << lg) - 1)) == 0 && j < P.n) aty[j] = acc;
@@ -1049,7 +1110,7 @@ __global__ void __launch_bounds__(256) k_spmv(SellDev S, const XT* x, AccT* y) {
     for (int s = gw; s < S.n_slices; s += nw) {
         const int4 sl = __ldg(S.slice + s);
         AccT acc = slice_dot<GK_GRID, AccT, V, XT>(S, vb, sl, lane, x);
-        if (!seg_finish<GK_GRID, AccT>(S, sl, lane, acc)) continue;
+        if (!seg_finish_last<AccT>(S, sl, lane, acc)) continue;
         const int lg = (int)((uint32_t)sl.y >> kLenBits);
         const int r = sl.x + (lane >> lg);
         if ((lane & ((1 << lg) - 1)) == 0 && r < S.n_rows) y[r] = acc;

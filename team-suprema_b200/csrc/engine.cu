@@ -141,6 +141,15 @@ struct EngineImpl {
         if (stream) cudaStreamDestroy(stream);
     }
 
+    // split-slice arrival counters start every product at zero (an abandoned
+    // solve may leave them counted up)
+    void clear_seg_counters(cudaStream_t st) {
+        for (const dev::SellDev* d : {&A, &AT})
+            if (d->seg_cnt)
+                cuda_ok(cudaMemsetAsync(d->seg_cnt, 0, sizeof(unsigned) * (size_t)(d == &A ? L.A : L.AT).n_groups(), st),
+                        "memset");
+    }
+
     dev::SellDev upload_sell(const SellHost& S) {
         dev::SellDev d{};
         d.n_rows = S.n_rows;
@@ -225,6 +234,10 @@ struct EngineImpl {
         const int64_t work = L.A.padded + L.AT.padded + 4 * ((int64_t)L.m + L.n);
         int ctas = (int)std::min<int64_t>(max_ctas, std::max<int64_t>(1, work / 16384));
         if (o.max_ctas > 0) ctas = std::min(ctas, o.max_ctas);
+        // split slices need the grid kernel with at least one warp per segment
+        // of the longest group (their completion waits on the other segments)
+        const int seg = std::max(L.A.seg_max, L.AT.seg_max);
+        if (seg > 0) ctas = std::min(max_ctas, std::max(ctas, std::max(2, (seg + dev::kWarps - 1) / dev::kWarps)));
         return std::max(1, ctas);
     }
 
@@ -269,6 +282,7 @@ struct EngineImpl {
     void launch(const dev::KParams<T>& P, const dev::GridArgs& ga, int ctas, cudaStream_t st) {
         cuda_ok(cudaMemsetAsync(bar, 0, sizeof(unsigned), st), "memset");
         cuda_ok(cudaMemsetAsync(abort_flag, 0, sizeof(int), st), "memset");
+        clear_seg_counters(st);
         if (ctas == 1 && !P.debug_delay_ns) {
             // x' and y' in shared memory when they fit next to the static part
             dev::GridArgs g1 = ga;
@@ -480,6 +494,7 @@ struct EngineImpl {
         cuda_ok(cudaMalloc(&dy, yd.size() * sizeof(double)), "cudaMalloc");
         cuda_ok(cudaMemcpy(dx, xd.data(), xd.size() * sizeof(double), cudaMemcpyHostToDevice), "H2D");
         const int blocks = std::max(1, std::min(sm_count * 8, (S.n_slices + 7) / 8));
+        clear_seg_counters(stream);
         if (S.n_slices > 0) {
             if (L.exact32) dev::k_spmv<double, float, double><<<blocks, 256, 0, stream>>>(S, dx, dy);
             else dev::k_spmv<double, double, double><<<blocks, 256, 0, stream>>>(S, dx, dy);
@@ -506,6 +521,7 @@ struct EngineImpl {
             else if (L.exact32) dev::k_spmv<double, float, double><<<blocks, 256, 0, st>>>(S, (const double*)x, (double*)y);
             else dev::k_spmv<double, double, double><<<blocks, 256, 0, st>>>(S, (const double*)x, (double*)y);
         };
+        clear_seg_counters(st);
         go();
         cuda_ok(cudaGetLastError(), "k_spmv");
         cuda_ok(cudaEventRecord(ev0, st), "event");

@@ -64,9 +64,13 @@ int pick_lanes(int64_t len, int lane_target) {
 // 8 sectors per step, padding included). Rows perm[i .. i+nr), g lanes per row.
 double slice_cost(const std::vector<int64_t>& ptr, const std::vector<int32_t>& idx, const std::vector<int32_t>& perm,
                   const std::vector<int32_t>& inv_col, int32_t i, int32_t nr, int g, int64_t len) {
-    double sectors = 8.0 * (double)len;
+    // at most 64 evenly spaced steps are counted and scaled to the slice
+    const int64_t stride = std::max<int64_t>(1, len / 64);
+    double sectors = 0.0;
+    int64_t samples = 0;
     uint32_t ids[32];
-    for (int64_t k = 0; k < len; ++k) {
+    for (int64_t k = 0; k < len; k += stride) {
+        ++samples;
         int cnt = 0;
         for (int lane = 0; lane < 32; ++lane) {
             const int32_t rl = lane / g, sub = lane % g;
@@ -83,7 +87,7 @@ double slice_cost(const std::vector<int64_t>& ptr, const std::vector<int32_t>& i
         std::sort(ids, ids + cnt);
         sectors += (double)(std::unique(ids, ids + cnt) - ids);
     }
-    return sectors;
+    return 8.0 * (double)len + (samples ? sectors * (double)len / (double)samples : 0.0);
 }
 
 // Builds the sliced format of the rows `perm` (device order) of a CSR whose
@@ -97,6 +101,7 @@ void build_sell(const std::vector<int64_t>& ptr, const std::vector<int32_t>& idx
     S.slice.clear();
     S.seg.clear();
     S.seg_slots = 0;
+    S.seg_max = 0;
     // pass 1: slice shapes
     struct Shape { int32_t row0, nrows, lg; int64_t len, blk; };
     std::vector<Shape> shapes;
@@ -107,6 +112,11 @@ void build_sell(const std::vector<int64_t>& ptr, const std::vector<int32_t>& idx
         for (int32_t t = 0; t < nr; ++t) lmax = std::max<int64_t>(lmax, ptr[perm[i + t] + 1] - ptr[perm[i + t]]);
         len = (lmax + g - 1) / g;
     };
+    // the tuned choice is kept for a shape class: rows of the same length in
+    // the same sigma window
+    const int window = bp.sigma_window > 0 ? bp.sigma_window : 1024;
+    int64_t class_len = -1, class_win = -1;
+    int class_g = 0;
     for (int32_t i = 0; i < rows;) {
         const int32_t r0 = perm[i];
         const int64_t rlen = ptr[r0 + 1] - ptr[r0];
@@ -114,7 +124,12 @@ void build_sell(const std::vector<int64_t>& ptr, const std::vector<int32_t>& idx
         int32_t nr = 0;
         int64_t len = 0;
         shape_of(i, g, nr, len);
-        if (bp.split && rlen >= bp.tune_len) {
+        if (bp.split && rlen >= bp.tune_len && rlen == class_len && i / window == class_win) {
+            if (class_g != g) {
+                g = class_g;
+                shape_of(i, g, nr, len);
+            }
+        } else if (bp.split && rlen >= bp.tune_len) {
             // long rows: the lanes-per-row whose slice touches the fewest
             // sectors per entry wins if it beats the length rule by 20%
             auto entries = [&](int32_t a, int32_t cnt) {
@@ -137,6 +152,9 @@ void build_sell(const std::vector<int64_t>& ptr, const std::vector<int32_t>& idx
                 g = best_g;
                 shape_of(i, g, nr, len);
             }
+            class_len = rlen;
+            class_win = i / window;
+            class_g = g;
         }
         if (len > (int64_t)kLenMask) fail(B2_ERR_UNSUPPORTED, "row too long for the sliced format");
         int lg = 0;
@@ -167,6 +185,7 @@ void build_sell(const std::vector<int64_t>& ptr, const std::vector<int32_t>& idx
             S.seg.push_back((int32_t)q_count);
             S.seg.push_back((int32_t)S.seg_slots);
             S.seg_slots += q_count;
+            S.seg_max = std::max<int32_t>(S.seg_max, (int32_t)q_count);
             for (int64_t q = 0; q < q_count; ++q) {
                 const int64_t l0 = q * seg_steps, l1 = std::min(sh.len, l0 + seg_steps);
                 S.slice.push_back(sh.row0);

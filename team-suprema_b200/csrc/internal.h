@@ -36,6 +36,7 @@ struct SellHost {
     // segment = group + 1 | segment << 24 (0: unsplit)
     std::vector<int32_t> seg;
     int64_t seg_slots = 0;            // segments in all groups (32 partial sums each)
+    int32_t seg_max = 0;              // most segments in one group
     int64_t n_slices() const { return (int64_t)slice.size() / 4; }
     int64_t n_groups() const { return (int64_t)seg.size() / 2; }
 };
@@ -71,7 +72,7 @@ struct BuildParams {
     // steps are split into segments that run on different warps
     bool split = false;
     int tune_len = 256;
-    int split_steps = 32;
+    int split_steps = 16;
 };
 
 // Validates the PDLP form and builds the device layout. Throws Error.
@@ -80,6 +81,10 @@ void build_layout(const b2_lp_view& U, const b2_lp_view& S, const double* Dr, co
 
 void scale_lp(const b2_lp_view& lp, int ruiz_passes, double* val_s, double* c_s, double* rL_s, double* rU_s,
               double* l_s, double* u_s, double* Dr, double* Dc);
+
+// The same scaling on the GPU, bit for bit (scale.cu).
+void scale_lp_gpu(const b2_lp_view& lp, int ruiz_passes, double* val_s, double* c_s, double* rL_s, double* rU_s,
+                  double* l_s, double* u_s, double* Dr, double* Dc);
 
 void gen_random_lp(int m, int n, int k, uint64_t seed, bool fp32_values, int32_t* row, int32_t* col, double* val,
                    double* c, double* rL, double* rU, double* l, double* u);

@@ -222,7 +222,8 @@ struct ServerImpl {
     b2_solve_opts o{};
     int device = 0, sm_count = 0, nt = 512, max_ctas = 0, max_clusters = 0, capacity = 0;
     BatchShape shape{};
-    cudaStream_t cs = nullptr, ds = nullptr;  // compute, copies
+    cudaStream_t cs = nullptr, cs2 = nullptr, ds = nullptr;  // compute (clusters, single CTAs), copies
+    cudaEvent_t ev_small = nullptr;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr, ev_copy = nullptr;
     cudaMemPool_t pool = nullptr;
     // device tables of the batched lane
@@ -271,6 +272,7 @@ struct ServerImpl {
         if (so.grid_nnz <= 0) so.grid_nnz = 4000000;
         if (so.grid_slice_ms <= 0) so.grid_slice_ms = 20.0;
         if (so.cluster_nnz == 0) so.cluster_nnz = 300000;
+        if (so.gpu_scale_nnz == 0) so.gpu_scale_nnz = 1000000;
         if (o.max_iterations < 0) fail(B2_ERR_INVALID, "max_iterations < 0");
         nt = o.batch_block == 128 || o.batch_block == 256 ? o.batch_block : 512;
         capacity = so.max_resident;
@@ -281,6 +283,8 @@ struct ServerImpl {
         cuda_ok(cudaDeviceGetAttribute(&sm_count, cudaDevAttrMultiProcessorCount, device), "attr");
         cuda_ok(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking), "cudaStreamCreate");
         cuda_ok(cudaStreamCreateWithFlags(&ds, cudaStreamNonBlocking), "cudaStreamCreate");
+        cuda_ok(cudaStreamCreateWithFlags(&cs2, cudaStreamNonBlocking), "cudaStreamCreate");
+        cuda_ok(cudaEventCreateWithFlags(&ev_small, cudaEventDisableTiming), "event");
         cuda_ok(cudaEventCreate(&ev0), "event");
         cuda_ok(cudaEventCreate(&ev1), "event");
         cuda_ok(cudaEventCreateWithFlags(&ev_copy, cudaEventDisableTiming), "event");
@@ -345,6 +349,8 @@ struct ServerImpl {
         if (ev0) cudaEventDestroy(ev0);
         if (ev1) cudaEventDestroy(ev1);
         if (ev_copy) cudaEventDestroy(ev_copy);
+        if (ev_small) cudaEventDestroy(ev_small);
+        if (cs2) cudaStreamDestroy(cs2);
         if (cs) cudaStreamDestroy(cs);
         if (ds) cudaStreamDestroy(ds);
     }
@@ -380,6 +386,7 @@ struct ServerImpl {
     }
 
     void prep_main() {
+        cudaSetDevice(device);  // large LPs are scaled on the GPU
         for (;;) {
             Request* r = nullptr;
             {
@@ -417,8 +424,13 @@ struct ServerImpl {
                      r.rL.data(), r.rU.data(), r.l.data(), r.u.data(), r.obj_offset};
         std::vector<double> val_s(r.val.size()), c_s(r.n), l_s(r.n), u_s(r.n), rL_s(r.m), rU_s(r.m), Dr(r.m),
             Dc(r.n);
-        scale_lp(U, 10, val_s.data(), c_s.data(), rL_s.data(), rU_s.data(), l_s.data(), u_s.data(), Dr.data(),
-                 Dc.data());
+        // the GPU computes the same scaling bit for bit; it pays off for large LPs
+        if (so.gpu_scale_nnz > 0 && (int64_t)r.val.size() >= so.gpu_scale_nnz)
+            scale_lp_gpu(U, 10, val_s.data(), c_s.data(), rL_s.data(), rU_s.data(), l_s.data(), u_s.data(),
+                         Dr.data(), Dc.data());
+        else
+            scale_lp(U, 10, val_s.data(), c_s.data(), rL_s.data(), rU_s.data(), l_s.data(), u_s.data(), Dr.data(),
+                     Dc.data());
         b2_lp_view S{r.m, r.n, (int64_t)r.val.size(), r.row.data(), r.col.data(), val_s.data(), c_s.data(),
                      rL_s.data(), rU_s.data(), l_s.data(), u_s.data(), r.obj_offset};
         BuildParams bp;
@@ -613,8 +625,24 @@ struct ServerImpl {
         cuda_ok(cudaMemsetAsync(B.next_large, 0, sizeof(unsigned), cs), "memset");
         cuda_ok(cudaMemsetAsync(B.t0, 0, sizeof(unsigned long long), cs), "memset");
         cuda_ok(cudaEventRecord(ev0, cs), "event");
-        if (B.n_large) batch_kernel_launch(B, true, nt, max_clusters, cs);
-        else batch_kernel_launch(B, false, nt, std::max(1, std::min(max_ctas, nq)), cs);
+        if (B.n_large) {
+            // clusters for the large LPs on up to 3/4 of the GPU, and beside
+            // them a one-CTA launch on the rest, so the small LPs never wait
+            // for the large ones; both take from the same queues
+            const int ncl = std::max(1, std::min(B.n_large, std::max(1, max_clusters * 3 / 4)));
+            batch_kernel_launch(B, true, nt, ncl, cs);
+            const int rest = max_ctas - ncl * dev::kMaxCluster;
+            if (n_small && rest > 0) {
+                cuda_ok(cudaStreamWaitEvent(cs2, ev0, 0), "wait");
+                dev::BatchArgs Bs = B;
+                Bs.n_large = 0;
+                batch_kernel_launch(Bs, false, nt, std::min(rest, n_small), cs2);
+                cuda_ok(cudaEventRecord(ev_small, cs2), "event");
+                cuda_ok(cudaStreamWaitEvent(cs, ev_small, 0), "wait");
+            }
+        } else {
+            batch_kernel_launch(B, false, nt, std::max(1, std::min(max_ctas, nq)), cs);
+        }
         cuda_ok(cudaEventRecord(ev1, cs), "event");
         // overlap: admit (and upload) new arrivals while the round runs
         for (;;) {
@@ -717,7 +745,9 @@ struct ServerImpl {
     void run_grid_slice() {
         Request* r = grid_resident.front();
         const auto t0 = Clock::now();
-        const bool ended = engine_slice(r->eng, o, so.grid_slice_ms, cs);
+        // short slices while batched LPs wait, long ones when the LP is alone
+        const double slice_ms = resident.empty() ? so.grid_slice_ms : std::min(so.grid_slice_ms, so.round_ms);
+        const bool ended = engine_slice(r->eng, o, slice_ms, cs);
         r->rounds++;
         {
             std::lock_guard<std::mutex> lk(mu);

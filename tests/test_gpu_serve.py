@@ -138,3 +138,23 @@ def test_malformed_request_fails_alone():
         st = srv.stats()
     assert r.converged and st["failed"] == 1 and st["completed"] == 1
     certified(U, r, G["fixtures"]["afiro"]["simplex"]["objective"])
+
+
+@pytest.mark.parametrize("cluster_nnz", [1, 3000])
+def test_cluster_lane_equals_batched_cluster_path(cluster_nnz):
+    """Served LPs above cluster_nnz stored entries run on 8-CTA clusters (beside
+    a one-CTA launch for the rest); each answer is the batched engine's on the
+    same path, bit for bit, however the rounds cut it."""
+    names, probs = fixture_problems()
+    with B.Server(round_ms=0.3, cluster_nnz=cluster_nnz, max_iterations=500000, tol=TOL) as srv:
+        out = [srv.wait(t, timeout_s=300.0) for t in [srv.submit(U) for (U, _, _, _) in probs]]
+    with B.Batch(probs) as bt:
+        res, _ = bt.solve(max_iterations=500000, tol=TOL, batch_cluster_nnz=cluster_nnz)
+        for i, (U, _, _, _) in enumerate(probs):
+            r, _ = out[i]
+            assert r.converged, names[i]
+            x, y = bt.solution(i)
+            assert r.iterations == res[i]["iterations"], names[i]
+            np.testing.assert_array_equal(r.x, x)
+            np.testing.assert_array_equal(r.y, y)
+            certified(U, r, G["fixtures"][names[i]]["simplex"]["objective"])
