@@ -163,6 +163,12 @@ def dist_max(x: float, world: int) -> float:
     return float(t.item())
 
 
+def job_rate(world: int, units_per_rank: float, max_ms: float) -> float:
+    """Whole-job throughput of `world` replicas that each processed
+    units_per_rank units, timed as the max over ranks (ms)."""
+    return world * units_per_rank / (max_ms / 1e3)
+
+
 def dist_barrier(world: int):
     if world > 1:
         import torch.distributed as dist
@@ -222,10 +228,11 @@ def workload_config(args, U, lp):
             "parallelism": f"replicas x{args.gpus}" if args.gpus > 1 else "single GPU"}
 
 
-def make_batch(B, name):
+def make_batch(B, name, count=0, m_hi=0):
     _, p = WORKLOADS[name]
     probs = []
-    for (m, n, k, seed) in B.batch_family_shapes(p["count"], p["seed"]):
+    shapes = B.batch_family_shapes(count or p["count"], p["seed"], m_hi=m_hi or 5000)
+    for (m, n, k, seed) in shapes:
         lp = B.gen_random_lp(m, n, k, seed, True)
         U, S, Dr, Dc, _ = B.prepare(lp)
         probs.append((U, S, Dr, Dc))
@@ -239,7 +246,7 @@ def batch_bench(args, world, rank, local):
     torch.cuda.set_device(local)
     prec = B.PREC_MIXED if args.precision == "mixed" else B.PREC_FP64
     t0 = time.time()
-    probs = make_batch(B, args.workload)
+    probs = make_batch(B, args.workload, args.batch_count, args.batch_mhi)
     t_prep = time.time() - t0
     t0 = time.time()
     bt = B.Batch(probs)
@@ -257,7 +264,7 @@ def batch_bench(args, world, rank, local):
     dist_barrier(world)
     ms_total = dist_max(sum(ms for _, ms in steps), world)
     n_lp = len(probs)
-    value = world * n_lp * args.steps / (ms_total / 1e3)
+    value = job_rate(world, n_lp * args.steps, ms_total)
     res = steps[-1][0]
     lat = sorted(r["device_ms"] for r in res)
     conv = sum(r["converged"] for r in res)
@@ -268,7 +275,8 @@ def batch_bench(args, world, rank, local):
             "warmup": args.warmup, "ms_per_step": ms_total / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64" if prec == B.PREC_MIXED else "f64",
             "data": "synthetic",
-            "config": {"workload": describe(args.workload), "lps": n_lp, "sum_m": info["sum_m"],
+            "config": {"workload": describe(args.workload), "lps": n_lp, "m_hi": args.batch_mhi or 5000,
+                       "sum_m": info["sum_m"],
                        "sum_n": info["sum_n"], "sum_nnz": info["sum_nnz"], "tol": args.tol,
                        "batch_block": bt.info()["threads_per_cta"], "batch_cluster_nnz": args.batch_cluster_nnz,
                        "parallelism": f"replicas x{world}" if world > 1 else "single GPU"},
@@ -336,7 +344,7 @@ def serve_bench(args, world, rank, local):
     first = min(info["submit_s"] for _, info in out)
     last = max(info["done_s"] for _, info in out)
     makespan = dist_max(last - first, world)
-    value = world * len(out) / makespan
+    value = job_rate(world, len(out), makespan * 1e3)
     conv = sum(r.converged for r, _ in out)
     worst = max(max(r.eps_P, r.eps_D, r.eps_G) for r, _ in out)
     lanes = [info["lane"] for _, info in out]
@@ -403,6 +411,8 @@ def main():
     ap.add_argument("--max-attempts", type=int, default=256, help="--mode solve: attempt limit")
     ap.add_argument("--reps", type=int, default=1, help="--mode spmv: timed launches per product")
     ap.add_argument("--batch-block", type=int, default=0, help="batch: threads per CTA (128/256/512, 0 auto)")
+    ap.add_argument("--batch-count", type=int, default=0, help="batch: LPs (0: 4096)")
+    ap.add_argument("--batch-mhi", type=int, default=0, help="batch: largest m of the family (0: 5000; profiling)")
     ap.add_argument("--serve-seconds", type=float, default=0.0, help="serve: arrival window (0: workload default)")
     ap.add_argument("--round-ms", type=float, default=5.0, help="serve: device time of one batched round")
     ap.add_argument("--batch-cluster-nnz", type=int, default=0,
@@ -456,7 +466,7 @@ def main():
     dist_barrier(world)
     ms_total = ev[0].elapsed_time(ev[1])
     ms_total = dist_max(ms_total, world)
-    value = world * args.steps / (ms_total / 1e3)
+    value = job_rate(world, args.steps, ms_total)
     lat = sorted(r.stats["device_ms"] for r in results)
 
     # roofline of the persistent kernel: algorithmic bytes of the accepted
@@ -491,7 +501,7 @@ def main():
         e2e_ms.append((time.perf_counter() - t1) * 1e3)
     e2e_ms = e2e_ms[1:]
     e2e_max = dist_max(sum(e2e_ms), world)
-    e2e_value = world * len(e2e_ms) / (e2e_max / 1e3)
+    e2e_value = job_rate(world, len(e2e_ms), e2e_max)
     h2d = info["device_bytes"]
     d2h = 8 * (m + n)
 

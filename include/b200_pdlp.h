@@ -273,7 +273,8 @@ int b2_server_submit(b2_server* s, const b2_lp_view* unscaled_form, int64_t* tic
 int b2_server_wait(b2_server* s, int64_t ticket, double timeout_s, double* x, double* y, b2_result* res,
                    b2_request_info* info);
 int b2_server_stats_get(b2_server* s, b2_server_stats* out);
-/* Stops the server: running LPs are abandoned, unclaimed results dropped. */
+/* Stops the server: running LPs stop at their next poll, unclaimed results are
+ * dropped. No other call on this server may be in progress or follow. */
 void b2_server_destroy(b2_server* s);
 
 /* ---- host-side preparation (product side, no GPU needed) ---------------- */

@@ -284,8 +284,8 @@ struct PoolOffsets {
 struct BatchImpl {
     int n = 0, sm_count = 0, max_ctas = 0, last_nt = 256;
     BatchShape shape{};
-    cudaStream_t stream = nullptr;
-    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    cudaStream_t stream = nullptr, stream2 = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr, ev_small = nullptr;
     std::vector<Layout> L;
     std::vector<PoolOffsets> off;
     std::vector<dev::LpDev> lps;  // host copy of the descriptors
@@ -316,6 +316,8 @@ struct BatchImpl {
         if (h_stop) cudaFreeHost(h_stop);
         if (ev0) cudaEventDestroy(ev0);
         if (ev1) cudaEventDestroy(ev1);
+        if (ev_small) cudaEventDestroy(ev_small);
+        if (stream2) cudaStreamDestroy(stream2);
         if (stream) cudaStreamDestroy(stream);
     }
 
@@ -377,6 +379,8 @@ struct BatchImpl {
         cuda_ok(cudaGetDevice(&device), "cudaGetDevice");
         cuda_ok(cudaDeviceGetAttribute(&sm_count, cudaDevAttrMultiProcessorCount, device), "attr");
         cuda_ok(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking), "cudaStreamCreate");
+        cuda_ok(cudaStreamCreateWithFlags(&stream2, cudaStreamNonBlocking), "cudaStreamCreate");
+        cuda_ok(cudaEventCreateWithFlags(&ev_small, cudaEventDisableTiming), "event");
         cuda_ok(cudaEventCreate(&ev0), "event");
         cuda_ok(cudaEventCreate(&ev1), "event");
 
@@ -551,9 +555,22 @@ struct BatchImpl {
         cuda_ok(cudaMemsetAsync(B.t0, 0, sizeof(unsigned long long), st), "memset");
         cuda_ok(cudaEventRecord(ev0, st), "event");
         if (!large_q.empty()) {
-            int ncl = shape.max_clusters_nt[ntx];
+            // clusters for the large LPs on at most half of the GPU, a one-CTA
+            // launch on the rest beside them (second stream); both take from
+            // the same queues, so the small LPs start at once
+            int ncl = std::min((int)large_q.size(), std::max(1, shape.max_clusters_nt[ntx] / 2));
             if (o.max_ctas > 0) ncl = std::max(1, std::min(ncl, o.max_ctas / dev::kMaxCluster));
             batch_kernel_launch(B, true, nt, ncl, st);
+            const int rest = (o.max_ctas > 0 ? std::min(o.max_ctas, shape.max_ctas_nt[ntx]) : shape.max_ctas_nt[ntx]) -
+                             ncl * dev::kMaxCluster;
+            if (!small_q.empty() && rest > 0) {
+                cuda_ok(cudaStreamWaitEvent(stream2, ev0, 0), "wait");
+                dev::BatchArgs Bs = B;
+                Bs.n_large = 0;
+                batch_kernel_launch(Bs, false, nt, std::min(rest, (int)small_q.size()), stream2);
+                cuda_ok(cudaEventRecord(ev_small, stream2), "event");
+                cuda_ok(cudaStreamWaitEvent(st, ev_small, 0), "wait");
+            }
         } else {
             const int ctas = std::max(1, std::min(shape.max_ctas_nt[ntx], o.max_ctas > 0 ? std::min(o.max_ctas, n) : n));
             batch_kernel_launch(B, false, nt, ctas, st);

@@ -173,20 +173,28 @@ __device__ __forceinline__ unsigned long long gtimer() {
     asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
     return t;
 }
-// Matrix streams: read-only for the kernel's lifetime, used once per pass.
+// Matrix streams: read-only for the kernel's lifetime. A whole-GPU pass
+// reads each entry once (no L1 allocation); a CTA that solves a small LP
+// alone reads its matrix every attempt, so there it may stay in L1.
+template <bool KEEP>
 __device__ __forceinline__ uint32_t ld_mat(const uint32_t* p) {
     uint32_t v;
-    asm("ld.global.nc.L1::no_allocate.u32 %0, [%1];" : "=r"(v) : "l"(p));
+    if (KEEP) asm("ld.global.nc.u32 %0, [%1];" : "=r"(v) : "l"(p));
+    else asm("ld.global.nc.L1::no_allocate.u32 %0, [%1];" : "=r"(v) : "l"(p));
     return v;
 }
+template <bool KEEP>
 __device__ __forceinline__ float ld_mat(const float* p) {
     float v;
-    asm("ld.global.nc.L1::no_allocate.f32 %0, [%1];" : "=f"(v) : "l"(p));
+    if (KEEP) asm("ld.global.nc.f32 %0, [%1];" : "=f"(v) : "l"(p));
+    else asm("ld.global.nc.L1::no_allocate.f32 %0, [%1];" : "=f"(v) : "l"(p));
     return v;
 }
+template <bool KEEP>
 __device__ __forceinline__ double ld_mat(const double* p) {
     double v;
-    asm("ld.global.nc.L1::no_allocate.f64 %0, [%1];" : "=d"(v) : "l"(p));
+    if (KEEP) asm("ld.global.nc.f64 %0, [%1];" : "=d"(v) : "l"(p));
+    else asm("ld.global.nc.L1::no_allocate.f64 %0, [%1];" : "=d"(v) : "l"(p));
     return v;
 }
 // Iterates are rewritten between passes, never read through the non-coherent
@@ -336,6 +344,7 @@ constexpr int kUnroll = B2_SLICE_UNROLL;
 
 template <int GK, class AccT, class V, class XT>
 __device__ __forceinline__ AccT slice_dot(const SellDev& S, const V* vbase, int4 sl, int lane, const XT* x) {
+    constexpr bool KEEP = GK == GK_CTA;
     const uint32_t len = (uint32_t)sl.y & kLenMask;
     const int lg = (int)((uint32_t)sl.y >> kLenBits);
     const size_t base = (size_t)(uint32_t)sl.z * 32u + (size_t)lane;
@@ -351,8 +360,8 @@ __device__ __forceinline__ AccT slice_dot(const SellDev& S, const V* vbase, int4
         AccT xx[kUnroll];
 #pragma unroll
         for (int q = 0; q < kUnroll; ++q) {
-            cc[q] = ld_mat(cp + 32 * q);
-            vv[q] = ld_mat(vp + 32 * q);
+            cc[q] = ld_mat<KEEP>(cp + 32 * q);
+            vv[q] = ld_mat<KEEP>(vp + 32 * q);
         }
 #pragma unroll
         for (int q = 0; q < kUnroll; ++q) xx[q] = (AccT)ld_it<GK>(x + cc[q]);
@@ -362,7 +371,7 @@ __device__ __forceinline__ AccT slice_dot(const SellDev& S, const V* vbase, int4
         vp += 32 * kUnroll;
     }
     for (; k < len; ++k) {
-        acc = fma((AccT)ld_mat(vp), (AccT)ld_it<GK>(x + ld_mat(cp)), acc);
+        acc = fma((AccT)ld_mat<KEEP>(vp), (AccT)ld_it<GK>(x + ld_mat<KEEP>(cp)), acc);
         cp += 32;
         vp += 32;
     }

@@ -158,3 +158,23 @@ def test_cluster_lane_equals_batched_cluster_path(cluster_nnz):
             np.testing.assert_array_equal(r.x, x)
             np.testing.assert_array_equal(r.y, y)
             certified(U, r, G["fixtures"][names[i]]["simplex"]["objective"])
+
+
+def test_pending_result_and_shutdown_with_requests_in_flight():
+    """wait() with a short timeout reports a running request as pending; closing
+    the server with requests in flight stops them at their next poll and
+    returns promptly."""
+    lps = [B.prepare(B.gen_random_lp(20_000, 60_000, 6, s, True))[0] for s in (1, 2, 3)]
+    srv = B.Server(round_ms=2.0, max_iterations=2_000_000, tol=1e-9)
+    ts = [srv.submit(U) for U in lps]
+    assert srv.wait(ts[0], timeout_s=0.05) is None
+    st = srv.stats()
+    assert st["submitted"] == 3 and st["completed"] == 0
+    t0 = time.perf_counter()
+    srv.close()
+    assert time.perf_counter() - t0 < 30.0
+    # a fresh server on the same device works afterwards
+    U, S, Dr, Dc = load_fixture("afiro")
+    with B.Server(round_ms=1.0) as s2:
+        r, _ = s2.wait(s2.submit(U), timeout_s=60.0)
+    certified(U, r, G["fixtures"]["afiro"]["simplex"]["objective"])
