@@ -48,6 +48,12 @@ WORKLOADS = {
 # count, which takes the reference's decisions (tests/test_gpu_solve.py).
 REF_ATTEMPTS = {"large": 143360, "medium": 73024, "small": 13888}
 
+# DRAM bytes (read + write) per attempt of the persistent solve kernel, from ncu captures of
+# 256-attempt solves of the workload (FP32 iterates, FP64 iterates); the roofline's `traffic`
+# scales them by the attempts of each timed launch. Command and figures:
+# profiles/k_pdlp_traffic_random_1M_cols.md.
+TRAFFIC_PER_ATTEMPT = {"large": (150.9e6, 203.9e6)}
+
 
 def describe(name):
     kind, p = WORKLOADS[name]
@@ -485,6 +491,12 @@ def main():
         tot_bytes += acc32 * algorithmic_bytes(m, n, z, 4) + acc64 * algorithmic_bytes(m, n, z, 8)
         tot_ms += r.stats["device_ms"]
     achieved = tot_bytes / (tot_ms / 1e3) / 1e9
+    launches = sum(1 + (1 if 0 < r.stats["fp32_attempts"] < r.iterations else 0) for r in results)
+    traffic = None
+    if args.workload in TRAFFIC_PER_ATTEMPT and args.precision == "mixed":
+        t32, t64 = TRAFFIC_PER_ATTEMPT[args.workload]
+        traffic = sum(r.stats["fp32_attempts"] * t32 + (r.iterations - r.stats["fp32_attempts"]) * t64
+                      for r in results) / launches
 
     # standalone SpMV (A x, FP32), the kernel every pass is built on
     spmv_ms = eng.spmv_bench(0, B.PREC_MIXED, 50, stream.cuda_stream)
@@ -535,15 +547,16 @@ def main():
                       "checks": r0.stats["checks"], "eps": [r0.eps_P, r0.eps_D, r0.eps_G],
                       "converged": r0.converged, "attempts_per_s": r0.iterations / (r0.stats["device_ms"] / 1e3)},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak_gbs, "unit": "GB/s",
-                         "frac": achieved / peak_gbs, "traffic": None,
+                         "frac": achieved / peak_gbs, "traffic": traffic,
+                         "algorithmic_bytes_per_launch": tot_bytes / launches,
+                         "traffic_note": "bytes per launch: ncu DRAM bytes per attempt x the launch's attempts"
+                                         if traffic else None,
                          "kernel": "k_pdlp (persistent solve)", "peak_source": peak_src},
             "spmv": {"A_gbs": spmv_gbs, "AT_gbs": spmv_t_gbs, "A_ms": spmv_ms, "AT_ms": spmv_t_ms,
                      "frac_A": spmv_gbs / peak_gbs, "frac_AT": spmv_t_gbs / peak_gbs},
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                     "ms_per_step": statistics.mean(e2e_ms)},
-            "cpu_baseline": cpu, "clocks": clocks, "gpu_launches": sum(
-                1 + (1 if r.stats["fp32_attempts"] and r.stats["fp32_attempts"] < r.iterations else 0)
-                for r in results),
+            "cpu_baseline": cpu, "clocks": clocks, "gpu_launches": launches,
             "prep_s": t_prep, "layout": {k: info[k] for k in ("ctas", "a_padded", "at_padded", "values_exact_fp32")},
         }
         print(json.dumps(line), flush=True)
