@@ -133,7 +133,7 @@ __global__ void __launch_bounds__(NT, 1024 / NT) k_pdlp_batch(const BatchArgs B)
     __shared__ KParams<double> Pd;
     __shared__ int s_inst, s_pos, s_exact;
     __shared__ unsigned long long s_deadline;
-    __shared__ double s_part[NSLOTS * kPartStride];
+    __shared__ double s_part[kCtaPartDoubles];
     const int tid = threadIdx.x, warp = tid >> 5;
     if (tid == 0) s_deadline = launch_deadline(B);
     __syncthreads();

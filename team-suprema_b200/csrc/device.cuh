@@ -46,9 +46,10 @@ namespace dev {
 
 constexpr int kBlock = 512;          // CTA size of the one-LP kernels (and the largest CTA size)
 constexpr int kWarps = kBlock / 32;
-constexpr int kPartStride = 32;  // doubles per CTA per reduction slot
+constexpr int kPartStride = 32;  // doubles per CTA (or per warp, one-CTA groups) per reduction slot
 constexpr int kMaxNV = 22;
 enum { SLOT_A = 0, SLOT_X = 1, SLOT_CK = 2, NSLOTS = 3 };
+constexpr int kCtaPartDoubles = NSLOTS * kWarps * kPartStride;  // a one-CTA group's shared partials
 enum { SEL_BEST = 0, SEL_CUR = 1, SEL_AVG = 2 };
 // MODE_START: cold start. MODE_RESUME: the FP64 phase takes over from the
 // FP32 phase (iterates widened, A x / A^T y recomputed). MODE_CONTINUE: the
@@ -157,7 +158,7 @@ struct Group {
     unsigned* bar;           // grid-barrier word (GK_GRID)
     int* abort;
     unsigned long long timeout_ns;
-    double* spart;           // GK_CTA: partial sums in shared memory, [NSLOTS][kPartStride]
+    double* spart;           // GK_CTA: warp partial sums in shared memory, [NSLOTS][kWarps][kPartStride]
     // global-timer deadline after which the solve yields at the next attempt
     // boundary (read on the group's first CTA only); 0: never
     unsigned long long yield_at = 0;
@@ -270,9 +271,30 @@ __device__ __forceinline__ bool group_sync(const Group& g) {
 
 // Per-CTA partial sums of NV values: k = 0..NV-1 go to index at + k of this
 // CTA's row of the slot. Fixed order: warp tree, then warps in order.
+//
+// One CTA alone (GK_CTA) keeps the warp partials themselves, [slot][warp][k]
+// in shared memory, and whoever reads the totals after the next barrier adds
+// the warps in order (cta_sum): the same sums, two fewer barriers an attempt.
+__device__ __forceinline__ double cta_sum(const Group& g, int slot, int k) {
+    double s = 0.0;
+    const int nwarps = blockDim.x >> 5;
+    for (int w = 0; w < nwarps; ++w) s += g.spart[(slot * kWarps + w) * kPartStride + k];
+    return s;
+}
+
 template <int NV, int GK>
 __device__ __forceinline__ void cta_partial_at(double (&v)[NV], const Group& g, int slot, int at, double* s_red) {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    if (GK == GK_CTA) {
+#pragma unroll
+        for (int k = 0; k < NV; ++k) {
+            double t = v[k];
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) t += __shfl_down_sync(0xffffffffu, t, o);
+            if (lane == 0) g.spart[(slot * kWarps + warp) * kPartStride + at + k] = t;
+        }
+        return;
+    }
 #pragma unroll
     for (int k = 0; k < NV; ++k) {
         double t = v[k];
@@ -285,8 +307,7 @@ __device__ __forceinline__ void cta_partial_at(double (&v)[NV], const Group& g, 
         double s = 0.0;
         const int nwarps = blockDim.x >> 5;
         for (int w = 0; w < nwarps; ++w) s += s_red[w * NV + threadIdx.x];
-        if (GK == GK_CTA) g.spart[slot * kPartStride + at + threadIdx.x] = s;
-        else g.part[((size_t)slot * g.size + g.rank) * kPartStride + at + threadIdx.x] = s;
+        g.part[((size_t)slot * g.size + g.rank) * kPartStride + at + threadIdx.x] = s;
     }
 }
 
@@ -299,7 +320,7 @@ __device__ __forceinline__ void cta_partial(double (&v)[NV], const Group& g, int
 template <int NV, int GK>
 __device__ __forceinline__ void group_totals(const Group& g, int slot, double* s_tot) {
     if (GK == GK_CTA) {
-        if (threadIdx.x < NV) s_tot[threadIdx.x] = g.spart[slot * kPartStride + threadIdx.x];
+        if (threadIdx.x < NV) s_tot[threadIdx.x] = cta_sum(g, slot, threadIdx.x);
         __syncthreads();
         return;
     }
@@ -318,9 +339,12 @@ __device__ __forceinline__ void group_totals(const Group& g, int slot, double* s
 template <int GK>
 __device__ __forceinline__ void step_totals(const Group& g, double* s_tot) {
     if (GK == GK_CTA) {
-        if (threadIdx.x < 3)
-            s_tot[threadIdx.x] = g.spart[(threadIdx.x < 2 ? SLOT_A : SLOT_X) * kPartStride + (threadIdx.x < 2 ? threadIdx.x : 0)];
-        __syncthreads();
+        // only thread 0 (the step decision) reads them: no barrier
+        if (threadIdx.x == 0) {
+            s_tot[0] = cta_sum(g, SLOT_A, 0);
+            s_tot[1] = cta_sum(g, SLOT_A, 1);
+            s_tot[2] = cta_sum(g, SLOT_X, 0);
+        }
         return;
     }
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -622,7 +646,7 @@ __device__ void pass_rows_check(const KParams<T>& P, const Ctl& c, const Group& 
         const int i = sl.x + (lane >> lg);
         if ((lane & ((1 << lg) - 1)) == 0 && i < P.m) {
             const double yc = (double)ld_it<GK>(y + i);
-            double ys = __ldcg(P.ysum + i);
+            double ys = ld_it<GK>(P.ysum + i);
             if (pend != 0.0) { ys += pend * yc; P.ysum[i] = ys; }
             const double ac = (double)ld_it<GK>(ax + i);
             const double aa = has_avg ? acc / wsum : ac;
@@ -659,7 +683,7 @@ __device__ void pass_cols_check(const KParams<T>& P, const Ctl& c, const Group& 
         const int j = sl.x + (lane >> lg);
         if ((lane & ((1 << lg) - 1)) == 0 && j < P.n) {
             const double xc = (double)ld_it<GK>(x + j), gc = (double)ld_it<GK>(aty + j);
-            const double xa = has_avg ? __ldcg(P.xsum + j) / wsum : xc;
+            const double xa = has_avg ? ld_it<GK>(P.xsum + j) / wsum : xc;
             const double ga = has_avg ? acc / wsum : gc;
             atya[j] = (T)ga;
             const double cc = __ldg(P.c + j), l = __ldg(P.l + j), u = __ldg(P.u + j);
@@ -684,7 +708,7 @@ __device__ void pass_after_check(const KParams<T>& P, const Ctl& c, const Group&
     for (int j = g.gt; j < P.n; j += g.nt) {
         const T xct = ld_it<GK>(x + j);
         const double xc = (double)xct;
-        const double xa = has_avg ? __ldcg(P.xsum + j) / wsum_old : xc;
+        const double xa = has_avg ? ld_it<GK>(P.xsum + j) / wsum_old : xc;
         if (best_sel == SEL_CUR) P.best_x[j] = xc;
         else if (best_sel == SEL_AVG) P.best_x[j] = xa;
         if (restart) {
@@ -701,7 +725,7 @@ __device__ void pass_after_check(const KParams<T>& P, const Ctl& c, const Group&
     for (int i = g.gt; i < P.m; i += g.nt) {
         const T yct = ld_it<GK>(y + i);
         const double yc = (double)yct;
-        const double ya = has_avg ? __ldcg(P.ysum + i) / wsum_old : yc;
+        const double ya = has_avg ? ld_it<GK>(P.ysum + i) / wsum_old : yc;
         if (best_sel == SEL_CUR) P.best_y[i] = yc;
         else if (best_sel == SEL_AVG) P.best_y[i] = ya;
         if (restart) {
@@ -837,7 +861,7 @@ template <int GK>
 __device__ bool yield_state(const KParamsBase& P, Ctl& s, const Group& g) {
     __shared__ double s_carry;
     if (GK == GK_CTA) {
-        if (threadIdx.x == 0) s_carry = g.spart[SLOT_X * kPartStride];
+        if (threadIdx.x == 0) s_carry = cta_sum(g, SLOT_X, 0);
     } else if (threadIdx.x < 32) {
         double v = 0.0;
         for (int b = threadIdx.x; b < g.size; b += 32) v += __ldcg(&g.part[((size_t)SLOT_X * g.size + b) * kPartStride]);
@@ -871,6 +895,7 @@ __device__ bool solve_body(const KParams<T>& P, const Group& g) {
     __shared__ double s_tot[kMaxNV];
     __shared__ int s_flag[4];
     __shared__ double s_wsum_old;
+    __shared__ double s_pw[2];
     const int tid = threadIdx.x, lane = tid & 31;
     constexpr bool kFP32 = sizeof(T) == 4;
 
@@ -898,7 +923,9 @@ __device__ bool solve_body(const KParams<T>& P, const Group& g) {
         // 0's partial and zeros for the others: the totals below then come
         // out bit-identical to the ones the uninterrupted solve would form.
         if (tid == 0) {
-            if (GK == GK_CTA) g.spart[SLOT_X * kPartStride] = s.dx2_carry;
+            if (GK == GK_CTA)
+                for (int w = 0; w < (int)(blockDim.x >> 5); ++w)
+                    g.spart[(SLOT_X * kWarps + w) * kPartStride] = w == 0 ? s.dx2_carry : 0.0;
             else g.part[((size_t)SLOT_X * g.size + g.rank) * kPartStride] = g.rank == 0 ? s.dx2_carry : 0.0;
         }
         if (sx)
@@ -977,6 +1004,14 @@ __device__ bool solve_body(const KParams<T>& P, const Group& g) {
     for (;;) {
         if (!check_pending) {
             // ---- rows pass of one attempt ----
+            // the step-size exponents (k+2)^-0.6 and (k+2)^-0.3 of this attempt
+            // (pdlp_algo.hpp:120-121) are computed off the critical path by a
+            // thread of the second warp while the pass runs
+            if (tid == (blockDim.x > 32 ? 32 : 0)) {
+                const double k1 = s.accepted + 2.0;
+                s_pw[0] = pow(k1, -0.6);
+                s_pw[1] = pow(k1, -0.3);
+            }
             const bool poll = (s.attempts & 15) == 0;
             int hstop = 0;
             if (poll && g.rank == 0 && tid == 0 && P.host_stop) hstop = *P.host_stop;
@@ -1001,9 +1036,8 @@ __device__ bool solve_body(const KParams<T>& P, const Group& g) {
                 const double dy2 = s_tot[0], inter = s_tot[1], dx2 = s_tot[2];
                 const double num = s.omega * dx2 + dy2 / s.omega;
                 const double eta_bar = fabs(inter) > 0 ? num / (2.0 * fabs(inter)) : kInfD;
-                const double k1 = s.accepted + 2.0;
-                const double grow = (1.0 + pow(k1, -0.6)) * s.eta;
-                const double eta_next = isfinite(eta_bar) ? fmin((1.0 - pow(k1, -0.3)) * eta_bar, grow) : grow;
+                const double grow = (1.0 + s_pw[0]) * s.eta;
+                const double eta_next = isfinite(eta_bar) ? fmin((1.0 - s_pw[1]) * eta_bar, grow) : grow;
                 s.pend_y = 0.0;  // applied by the rows pass just finished
                 s.pend_x = 0.0;
                 if (s.eta <= eta_bar) {
@@ -1094,12 +1128,12 @@ __device__ bool solve_body(const KParams<T>& P, const Group& g) {
         const double wsum = s.wsum;
         for (int j = g.gt; j < P.n; j += g.nt) {
             const double v = sel == SEL_CUR ? (double)ld_it<GK>(x + j)
-                             : sel == SEL_AVG ? __ldcg(P.xsum + j) / wsum : __ldcg(P.best_x + j);
+                             : sel == SEL_AVG ? ld_it<GK>(P.xsum + j) / wsum : ld_it<GK>(P.best_x + j);
             P.out_x[P.perm_c[j]] = v;
         }
         for (int i = g.gt; i < P.m; i += g.nt) {
             const double v = sel == SEL_CUR ? (double)ld_it<GK>(y + i)
-                             : sel == SEL_AVG ? __ldcg(P.ysum + i) / wsum : __ldcg(P.best_y + i);
+                             : sel == SEL_AVG ? ld_it<GK>(P.ysum + i) / wsum : ld_it<GK>(P.best_y + i);
             P.out_y[P.perm_r[i]] = v;
         }
         __syncthreads();

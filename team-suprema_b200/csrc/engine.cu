@@ -53,7 +53,7 @@ __global__ void __launch_bounds__(kBlock, 2) k_pdlp(const KParams<T> P, const Gr
 // fences, partial sums in shared memory).
 template <class T, class V>
 __global__ void __launch_bounds__(kBlock, 2) k_pdlp_cta(const KParams<T> P, const GridArgs ga) {
-    __shared__ double s_part[NSLOTS * kPartStride];
+    __shared__ double s_part[kCtaPartDoubles];
     extern __shared__ __align__(16) unsigned char s_vec[];
     Group g;
     g.rank = 0;

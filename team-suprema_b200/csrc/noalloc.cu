@@ -44,7 +44,7 @@ static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocBytes];
 // The same one-CTA solve as k_pdlp_cta in engine.cu.
 template <class T, class V>
 __global__ void __launch_bounds__(kBlock, 2) k_pdlp_cta_static(const KParams<T> P, double* bcast, int* abort_word) {
-    __shared__ double s_part[NSLOTS * kPartStride];
+    __shared__ double s_part[kCtaPartDoubles];
     Group g;
     g.rank = 0;
     g.size = 1;
