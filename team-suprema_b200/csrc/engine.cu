@@ -12,6 +12,7 @@
 #include <limits>
 #include <memory>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "batch.h"
@@ -186,6 +187,7 @@ struct EngineImpl {
         bp.lane_target = o.lane_target;
         bp.sigma_window = o.sigma_window;
         bp.split = true;  // the whole GPU works on this LP: tune and split long rows
+        bp.threads = (int)std::max(1u, std::min(8u, std::thread::hardware_concurrency()));
         build_layout(U, S, Dr, Dc, bp, L);
         create_device();
     }

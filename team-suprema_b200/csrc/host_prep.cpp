@@ -10,6 +10,7 @@
 #include <limits>
 #include <numeric>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "internal.h"
@@ -169,14 +170,13 @@ void build_sell(const std::vector<int64_t>& ptr, const std::vector<int32_t>& idx
     S.val32.assign((size_t)S.padded, 0.0f);
     if (keep64) S.val64.assign((size_t)S.padded, 0.0);
     else S.val64.clear();
-    // pass 2: fill; a slice longer than split_steps becomes segments of at
+    // slice records: a slice longer than split_steps becomes segments of at
     // most that many steps (at most 255 of them), consecutive slice records
     // over the same rows and storage
     const int64_t split_at = bp.split ? std::max(1, bp.split_steps) : INT64_MAX;
     S.slice.reserve(shapes.size() * 4);
     for (size_t s = 0; s < shapes.size(); ++s) {
         const Shape& sh = shapes[s];
-        const int g = 1 << sh.lg;
         if (sh.len > split_at) {
             const int64_t seg_steps = std::max<int64_t>(split_at, (sh.len + 254) / 255);
             const int64_t q_count = (sh.len + seg_steps - 1) / seg_steps;
@@ -199,24 +199,44 @@ void build_sell(const std::vector<int64_t>& ptr, const std::vector<int32_t>& idx
             S.slice.push_back((int32_t)(uint32_t)sh.blk);
             S.slice.push_back(0);
         }
-        for (int lane = 0; lane < 32; ++lane) {
-            const int32_t rl = lane / g, sub = lane % g;
-            uint32_t last_col = 0;
-            int64_t k = 0;
-            if (rl < sh.nrows) {
-                const int32_t r = perm[sh.row0 + rl];
-                const int64_t b = ptr[r], e = ptr[r + 1];
-                if (e > b) last_col = (uint32_t)inv_col[idx[b]];
-                for (int64_t p = b + sub; p < e; p += g, ++k) {
-                    const size_t pos = (size_t)((sh.blk + k) * 32 + lane);
-                    last_col = (uint32_t)inv_col[idx[p]];
-                    S.col[pos] = last_col;
-                    S.val32[pos] = (float)val[p];
-                    if (keep64) S.val64[pos] = val[p];
+    }
+    // fill: every slice owns its storage range, so ranges of slices fill in
+    // parallel (the result does not depend on the thread count)
+    auto fill = [&](size_t s0, size_t s1) {
+        for (size_t s = s0; s < s1; ++s) {
+            const Shape& sh = shapes[s];
+            const int g = 1 << sh.lg;
+            for (int lane = 0; lane < 32; ++lane) {
+                const int32_t rl = lane / g, sub = lane % g;
+                uint32_t last_col = 0;
+                int64_t k = 0;
+                if (rl < sh.nrows) {
+                    const int32_t r = perm[sh.row0 + rl];
+                    const int64_t b = ptr[r], e = ptr[r + 1];
+                    if (e > b) last_col = (uint32_t)inv_col[idx[b]];
+                    for (int64_t p = b + sub; p < e; p += g, ++k) {
+                        const size_t pos = (size_t)((sh.blk + k) * 32 + lane);
+                        last_col = (uint32_t)inv_col[idx[p]];
+                        S.col[pos] = last_col;
+                        S.val32[pos] = (float)val[p];
+                        if (keep64) S.val64[pos] = val[p];
+                    }
                 }
+                for (; k < sh.len; ++k) S.col[(size_t)((sh.blk + k) * 32 + lane)] = last_col;  // value stays 0
             }
-            for (; k < sh.len; ++k) S.col[(size_t)((sh.blk + k) * 32 + lane)] = last_col;  // value stays 0
         }
+    };
+    const size_t nth = std::max<size_t>(1, std::min<size_t>((size_t)std::max(1, bp.threads), shapes.size() / 256 + 1));
+    if (nth <= 1) {
+        fill(0, shapes.size());
+    } else {
+        std::vector<std::thread> pool;
+        const size_t per = (shapes.size() + nth - 1) / nth;
+        for (size_t t = 0; t < nth; ++t) {
+            const size_t s0 = std::min(shapes.size(), t * per), s1 = std::min(shapes.size(), s0 + per);
+            pool.emplace_back(fill, s0, s1);
+        }
+        for (auto& th : pool) th.join();
     }
 }
 
@@ -266,8 +286,14 @@ void build_layout(const b2_lp_view& U, const b2_lp_view& S, const double* Dr, co
     std::vector<int64_t> aptr, tptr;
     std::vector<int32_t> aidx, tidx;
     std::vector<double> aval, tval;
-    coo_to_csr(m, nnz, U.row_idx, U.col_idx, U.val, aptr, aidx, aval);
-    coo_to_csr(n, nnz, U.col_idx, U.row_idx, U.val, tptr, tidx, tval);
+    {
+        // A and A^T are independent: two threads when the caller allows
+        std::thread ta;
+        if (bp.threads > 1) ta = std::thread([&] { coo_to_csr(m, nnz, U.row_idx, U.col_idx, U.val, aptr, aidx, aval); });
+        else coo_to_csr(m, nnz, U.row_idx, U.col_idx, U.val, aptr, aidx, aval);
+        coo_to_csr(n, nnz, U.col_idx, U.row_idx, U.val, tptr, tidx, tval);
+        if (ta.joinable()) ta.join();
+    }
 
     L.exact32 = true;
     for (int64_t k = 0; k < nnz; ++k)
@@ -282,8 +308,16 @@ void build_layout(const b2_lp_view& U, const b2_lp_view& S, const double* Dr, co
     for (int32_t i = 0; i < m; ++i) L.inv_r[L.perm_r[i]] = i;
     for (int32_t j = 0; j < n; ++j) L.inv_c[L.perm_c[j]] = j;
 
-    build_sell(aptr, aidx, aval, L.perm_r, L.inv_c, n, target, !L.exact32, bp, L.A);
-    build_sell(tptr, tidx, tval, L.perm_c, L.inv_r, m, target, !L.exact32, bp, L.AT);
+    if (bp.threads > 1) {
+        BuildParams half = bp;
+        half.threads = std::max(1, bp.threads / 2);
+        std::thread ta([&] { build_sell(aptr, aidx, aval, L.perm_r, L.inv_c, n, target, !L.exact32, half, L.A); });
+        build_sell(tptr, tidx, tval, L.perm_c, L.inv_r, m, target, !L.exact32, half, L.AT);
+        ta.join();
+    } else {
+        build_sell(aptr, aidx, aval, L.perm_r, L.inv_c, n, target, !L.exact32, bp, L.A);
+        build_sell(tptr, tidx, tval, L.perm_c, L.inv_r, m, target, !L.exact32, bp, L.AT);
+    }
 
     L.b.resize(m); L.rU.resize(m); L.dr2.resize(m);
     for (int32_t i = 0; i < m; ++i) {

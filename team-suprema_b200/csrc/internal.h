@@ -73,6 +73,7 @@ struct BuildParams {
     bool split = false;
     int tune_len = 256;
     int split_steps = 16;
+    int threads = 1;        // host threads for the layout (the one-LP engine uses several)
 };
 
 // Validates the PDLP form and builds the device layout. Throws Error.
