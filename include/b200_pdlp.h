@@ -75,7 +75,7 @@ typedef struct b2_solve_opts {
     int32_t debug_delay_us;   /* test hook: CTA 0 reaches its first barrier this late (bounded),
                                  so a short barrier_timeout_s exercises the timeout path   */
     int32_t batch_cluster_nnz;/* batches: LPs with at least this many stored entries (A and A^T)
-                                 are solved by a cluster of 8 CTAs; <= 0: never (default)     */
+                                 are solved by a cluster of 16 CTAs; <= 0: never (default)     */
     int32_t batch_block;      /* batches: threads per CTA, 128, 256 or 512; 0: auto (512)     */
 } b2_solve_opts;
 
@@ -239,7 +239,7 @@ typedef struct b2_server_opts {
     int64_t grid_nnz;         /* nonzeros from which an LP takes the whole-GPU lane; <= 0: 4,000,000 */
     double grid_slice_ms;     /* device time of one whole-GPU slice; <= 0: 20 ms        */
     int64_t cluster_nnz;      /* stored entries (A and A^T) from which a batched LP is solved by
-                                 a cluster of 8 CTAs; 0: 300,000; < 0: never             */
+                                 a cluster of 16 CTAs; 0: 300,000; < 0: never             */
     int64_t gpu_scale_nnz;    /* nonzeros from which an LP is scaled on the GPU (b2_scale_gpu,
                                  the same bits); 0: 1,000,000; < 0: never                */
 } b2_server_opts;
@@ -266,6 +266,10 @@ int b2_server_create(const b2_server_opts* sopts, const b2_solve_opts* opts, b2_
 /* Submits one LP in unscaled PDLP form (as solve_pdhg_gpu's unscaled_form: rows
  * `=` or `>=`); the server copies it and returns at once with a ticket. */
 int b2_server_submit(b2_server* s, const b2_lp_view* unscaled_form, int64_t* ticket);
+/* Submits an LP stored in the binary request format (b2_lp_write); the file
+ * is read and checked on the server's preparation threads, not the caller's.
+ * A file that cannot be read or is malformed fails its ticket. */
+int b2_server_submit_file(b2_server* s, const char* path, int64_t* ticket);
 /* Waits up to timeout_s seconds (< 0: no limit) for a ticket. On B2_OK the
  * result is handed over (x: n, y: m in unscaled PDLP-form space, any may be
  * NULL) and the ticket is forgotten; B2_ERR_PENDING: not finished yet. A
@@ -291,6 +295,16 @@ int b2_scale(const b2_lp_view* lp, int32_t ruiz_passes, double* val_s, double* c
  * does. For ingest of large LPs, whose host scaling takes seconds. */
 int b2_scale_gpu(const b2_lp_view* lp, int32_t ruiz_passes, double* val_s, double* c_s, double* rL_s,
                  double* rU_s, double* l_s, double* u_s, double* Dr, double* Dc);
+
+/* Binary LP request format (no counterpart in the reference, which reads MPS
+ * text, src/mps_reader.cpp:66-308): the LP of a b2_lp_view with A in CSR
+ * (format in team-suprema_b200/csrc/lp_io.cpp). b2_lp_read_dims gives the sizes
+ * to allocate; b2_lp_read fills caller buffers (row/col/val: nnz, c/l/u: n,
+ * rL/rU: m) with A in COO, rows in order. A malformed file is B2_ERR_INVALID. */
+int b2_lp_write(const char* path, const b2_lp_view* lp);
+int b2_lp_read_dims(const char* path, int32_t* m, int32_t* n, int64_t* nnz);
+int b2_lp_read(const char* path, int32_t* row, int32_t* col, double* val, double* c, double* rL, double* rU,
+               double* l, double* u, double* obj_offset);
 
 /* Synthetic LPs of the benchmark shapes (seeded, deterministic):
  * equality-form LP min c'x, Ax = b, 0 <= x <= 10, `k` distinct uniform rows per

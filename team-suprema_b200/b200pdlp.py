@@ -42,7 +42,8 @@ EXPORTED = [
     "b2_engine_destroy", "b2_engine_get_info", "b2_engine_spmv", "b2_engine_spmv_bench", "b2_engine_trace",
     "b2_batch_create", "b2_batch_solve", "b2_batch_get_solution", "b2_batch_get_info", "b2_batch_spmv",
     "b2_batch_destroy",
-    "b2_server_create", "b2_server_submit", "b2_server_wait", "b2_server_stats_get", "b2_server_destroy",
+    "b2_server_create", "b2_server_submit", "b2_server_submit_file", "b2_server_wait", "b2_server_stats_get",
+    "b2_server_destroy", "b2_lp_write", "b2_lp_read_dims", "b2_lp_read",
     "b2_scale", "b2_scale_gpu",
     "b2_gen_random_lp", "b2_gen_transport", "b2_last_error", "b2_version",
 ]
@@ -152,6 +153,10 @@ def lib():
             L.b2_batch_destroy.restype = None
             L.b2_server_create.argtypes = [C.POINTER(ServerOpts), C.POINTER(SolveOpts), C.POINTER(vp)]
             L.b2_server_submit.argtypes = [vp, C.POINTER(_LPView), C.POINTER(i64)]
+            L.b2_server_submit_file.argtypes = [vp, C.c_char_p, C.POINTER(i64)]
+            L.b2_lp_write.argtypes = [C.c_char_p, C.POINTER(_LPView)]
+            L.b2_lp_read_dims.argtypes = [C.c_char_p, C.POINTER(i32), C.POINTER(i32), C.POINTER(i64)]
+            L.b2_lp_read.argtypes = [C.c_char_p] + [vp] * 8 + [C.POINTER(f64)]
             L.b2_server_wait.argtypes = [vp, i64, f64, vp, vp, C.POINTER(_Result), C.POINTER(RequestInfo)]
             L.b2_server_stats_get.argtypes = [vp, C.POINTER(ServerStats)]
             L.b2_server_destroy.argtypes = [vp]
@@ -499,6 +504,14 @@ class Server:
         self._dims[t.value] = (U.m, U.n)
         return t.value
 
+    def submit_file(self, path: str) -> int:
+        """Submits an LP stored with write_lp; the server reads it on its own threads."""
+        m, n, _ = lp_file_dims(path)
+        t = C.c_int64()
+        _check(lib().b2_server_submit_file(self._h, os.fsencode(path), C.byref(t)))
+        self._dims[t.value] = (m, n)
+        return t.value
+
     def wait(self, ticket: int, timeout_s: float = -1.0):
         """(PdlpResult, info) once the ticket is done; None if timeout_s passed first."""
         m, n = self._dims[ticket]
@@ -518,6 +531,29 @@ class Server:
         st = ServerStats()
         _check(lib().b2_server_stats_get(self._h, C.byref(st)))
         return {k: getattr(st, k) for k, _ in ServerStats._fields_}
+
+
+# ---------------------------------------------------------- request files
+def write_lp(path: str, lp: RangedLP):
+    """Stores an LP in the binary request format (A in CSR; b2_lp_write)."""
+    lp = RangedLP.like(lp)
+    _check(lib().b2_lp_write(os.fsencode(path), C.byref(lp.view())))
+
+
+def lp_file_dims(path: str):
+    m, n, z = C.c_int32(), C.c_int32(), C.c_int64()
+    _check(lib().b2_lp_read_dims(os.fsencode(path), C.byref(m), C.byref(n), C.byref(z)))
+    return m.value, n.value, z.value
+
+
+def read_lp(path: str) -> RangedLP:
+    """Reads a request file back (A in COO, rows in order)."""
+    m, n, z = lp_file_dims(path)
+    row = np.zeros(max(z, 1), np.int32); col = np.zeros(max(z, 1), np.int32); val = np.zeros(max(z, 1))
+    c = np.zeros(max(n, 1)); l = np.zeros(max(n, 1)); u = np.zeros(max(n, 1))
+    rL = np.zeros(max(m, 1)); rU = np.zeros(max(m, 1)); off = C.c_double()
+    _check(lib().b2_lp_read(os.fsencode(path), *[_ptr(a) for a in (row, col, val, c, rL, rU, l, u)], C.byref(off)))
+    return RangedLP(m, n, row[:z], col[:z], val[:z], c[:n], rL[:m], rU[:m], l[:n], u[:n], off.value)
 
 
 # ------------------------------------------------------------- host-side prep

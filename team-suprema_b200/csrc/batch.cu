@@ -256,6 +256,10 @@ void batch_kernel_shape(int sm_count, BatchShape& out) {
         cudaLaunchAttribute at[1];
         cluster_cfg(cfg, at, 1, nt, nullptr);
         int ncl = 0;
+        // clusters of 16 exceed the portable size of 8: allowed per kernel
+        if (cudaFuncSetAttribute(batch_kernel(dev::kMaxCluster, nt), cudaFuncAttributeNonPortableClusterSizeAllowed, 1) !=
+            cudaSuccess)
+            cudaGetLastError();
         if (cudaOccupancyMaxActiveClusters(&ncl, batch_kernel(dev::kMaxCluster, nt), &cfg) != cudaSuccess) {
             cudaGetLastError();
             ncl = 0;

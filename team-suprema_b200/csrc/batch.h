@@ -6,7 +6,7 @@
 namespace b2 {
 namespace dev {
 
-constexpr int kMaxCluster = 8;
+constexpr int kMaxCluster = 16;  // CTAs per cluster (non-portable size: enabled per kernel)
 constexpr int kClusterScratch = NSLOTS * kMaxCluster * kPartStride + 8;
 
 struct BatchArgs {
@@ -32,7 +32,7 @@ struct BatchArgs {
 
 }  // namespace dev
 
-// Co-resident CTAs (CL = 1) and clusters of kMaxCluster (CL = 8) of the
+// Co-resident CTAs (CL = 1) and clusters of kMaxCluster (CL = 16) of the
 // batched kernel for CTAs of 128, 256 and 512 threads.
 struct BatchShape {
     int max_ctas_nt[3];

@@ -188,6 +188,45 @@ int b2_server_submit(b2_server* s, const b2_lp_view* U, int64_t* ticket) {
     });
 }
 
+int b2_server_submit_file(b2_server* s, const char* path, int64_t* ticket) {
+    return b2::guarded([&] {
+        if (!s || !path || !ticket) b2::fail(B2_ERR_INVALID, "null argument");
+        *ticket = b2::server_submit_file(s->impl, path);
+    });
+}
+
+int b2_lp_write(const char* path, const b2_lp_view* lp) {
+    return b2::guarded([&] {
+        if (!path || !lp) b2::fail(B2_ERR_INVALID, "null argument");
+        b2::lp_write(path, *lp);
+    });
+}
+
+int b2_lp_read_dims(const char* path, int32_t* m, int32_t* n, int64_t* nnz) {
+    return b2::guarded([&] {
+        if (!path || !m || !n || !nnz) b2::fail(B2_ERR_INVALID, "null argument");
+        b2::lp_read_dims(path, m, n, nnz);
+    });
+}
+
+int b2_lp_read(const char* path, int32_t* row, int32_t* col, double* val, double* c, double* rL, double* rU,
+               double* l, double* u, double* obj_offset) {
+    return b2::guarded([&] {
+        if (!path) b2::fail(B2_ERR_INVALID, "null argument");
+        b2::LpArrays a;
+        b2::lp_read(path, a);
+        auto cp = [](auto* dst, const auto& v) {
+            if (!v.empty()) {
+                if (!dst) b2::fail(B2_ERR_INVALID, "null output buffer");
+                std::memcpy(dst, v.data(), v.size() * sizeof(v[0]));
+            }
+        };
+        cp(row, a.row); cp(col, a.col); cp(val, a.val);
+        cp(c, a.c); cp(l, a.l); cp(u, a.u); cp(rL, a.rL); cp(rU, a.rU);
+        if (obj_offset) *obj_offset = a.obj_offset;
+    });
+}
+
 int b2_server_wait(b2_server* s, int64_t ticket, double timeout_s, double* x, double* y, b2_result* res,
                    b2_request_info* info) {
     int rc = B2_OK;

@@ -542,16 +542,21 @@ __device__ __forceinline__ void kkt_col(double l, double u, double cc, double x,
 // Primal step of one column (pdlp_algo.hpp:110 / src/pdlp.cpp:122-124) in
 // unscaled coordinates: x' = clamp(x - tau Dc^2 (c - A^T y), l, u).
 template <class T>
-__device__ __forceinline__ void primal_col(const KParams<T>& P, int j, T xv, double g, double tau, T* xn,
-                                           double& dx2, T* xs) {
-    const double w = __ldg(P.dc2 + j);
-    double v = (double)xv - tau * w * (__ldg(P.c + j) - g);
-    v = fmin(fmax(v, __ldg(P.l + j)), __ldg(P.u + j));
+__device__ __forceinline__ void primal_col_w(int j, T xv, double g, double tau, T* xn, double& dx2, T* xs,
+                                             double w, double cj, double lj, double uj) {
+    double v = (double)xv - tau * w * (cj - g);
+    v = fmin(fmax(v, lj), uj);
     const T vt = (T)v;
     xn[j] = vt;
     if (xs) xs[j] = vt;  // the copy the next A x' gathers from
     const double d = (double)vt - (double)xv;
     dx2 += d * d / w;
+}
+
+template <class T>
+__device__ __forceinline__ void primal_col(const KParams<T>& P, int j, T xv, double g, double tau, T* xn,
+                                           double& dx2, T* xs) {
+    primal_col_w<T>(j, xv, g, tau, xn, dx2, xs, __ldg(P.dc2 + j), __ldg(P.c + j), __ldg(P.l + j), __ldg(P.u + j));
 }
 
 // --------------------------------------------------------------- passes
@@ -570,15 +575,24 @@ __device__ void pass_rows_step(const KParams<T>& P, const Ctl& c, const Group& g
     const V* vb = vals<V>(P.A);
     for (int s = g.gw; s < P.A.n_slices; s += g.nw) {
         const int4 sl = __ldg(P.A.slice + s);
-        T acc = slice_dot<GK, T, V, T>(P.A, vb, sl, lane, xn);
-        if (!seg_finish<GK, T>(P.A, sl, lane, acc, g)) continue;
         const int lg = (int)((uint32_t)sl.y >> kLenBits);
         const int row = sl.x + (lane >> lg);
-        if ((lane & ((1 << lg) - 1)) == 0 && row < P.m) {
-            const T yv = ld_it<GK>(y + row), axv = ld_it<GK>(ax + row);
-            const double w = __ldg(P.dr2 + row);
+        const bool lead = (lane & ((1 << lg) - 1)) == 0 && row < P.m;
+        // the epilogue's operands are loaded before the product, so their
+        // latency hides behind its gathers
+        T yv = T(0), axv = T(0);
+        double w = 0.0, brow = 0.0;
+        if (lead) {
+            yv = ld_it<GK>(y + row);
+            axv = ld_it<GK>(ax + row);
+            w = __ldg(P.dr2 + row);
+            brow = __ldg(P.b + row);
+        }
+        T acc = slice_dot<GK, T, V, T>(P.A, vb, sl, lane, xn);
+        if (!seg_finish<GK, T>(P.A, sl, lane, acc, g)) continue;
+        if (lead) {
             const double aw = fabs(w);
-            double nv = (double)yv + sigma * aw * (__ldg(P.b + row) - (2.0 * (double)acc - (double)axv));
+            double nv = (double)yv + sigma * aw * (brow - (2.0 * (double)acc - (double)axv));
             if (w < 0.0 && nv < 0.0) nv = 0.0;
             const T nt = (T)nv;
             yn[row] = nt;
@@ -605,15 +619,25 @@ __device__ void pass_cols_step(const KParams<T>& P, const Ctl& c, const Group& g
         const V* vb = vals<V>(P.AT);
         for (int s = g.gw; s < P.AT.n_slices; s += g.nw) {
             const int4 sl = __ldg(P.AT.slice + s);
-            T acc = slice_dot<GK, T, V, T>(P.AT, vb, sl, lane, y);
-            if (!seg_finish<GK, T>(P.AT, sl, lane, acc, g)) continue;
             const int lg = (int)((uint32_t)sl.y >> kLenBits);
             const int j = sl.x + (lane >> lg);
-            if ((lane & ((1 << lg) - 1)) == 0 && j < P.n) {
+            const bool lead = (lane & ((1 << lg) - 1)) == 0 && j < P.n;
+            // the primal step's operands are loaded before the product
+            T xv = T(0);
+            double w = 1.0, cj = 0.0, lj = 0.0, uj = 0.0;
+            if (lead) {
+                xv = ld_it<GK>(x + j);
+                w = __ldg(P.dc2 + j);
+                cj = __ldg(P.c + j);
+                lj = __ldg(P.l + j);
+                uj = __ldg(P.u + j);
+            }
+            T acc = slice_dot<GK, T, V, T>(P.AT, vb, sl, lane, y);
+            if (!seg_finish<GK, T>(P.AT, sl, lane, acc, g)) continue;
+            if (lead) {
                 aty[j] = acc;
-                const T xv = ld_it<GK>(x + j);
                 if (pend != 0.0) P.xsum[j] += pend * (double)xv;
-                primal_col<T>(P, j, xv, (double)acc, tau, xn, dx2, sx);
+                primal_col_w<T>(j, xv, (double)acc, tau, xn, dx2, sx, w, cj, lj, uj);
             }
         }
     } else {

@@ -92,6 +92,19 @@ void gen_random_lp(int m, int n, int k, uint64_t seed, bool fp32_values, int32_t
 void gen_transport(int S, int D, uint64_t seed, int32_t* row, int32_t* col, double* val, double* c, double* rL,
                    double* rU, double* l, double* u);
 
+// An LP held in owned arrays (COO), e.g. as read from a request file.
+struct LpArrays {
+    int32_t m = 0, n = 0;
+    std::vector<int32_t> row, col;
+    std::vector<double> val, c, rL, rU, l, u;
+    double obj_offset = 0.0;
+};
+
+// The binary request format (lp_io.cpp). All functions throw Error.
+void lp_write(const std::string& path, const b2_lp_view& lp);
+void lp_read_dims(const std::string& path, int32_t* m, int32_t* n, int64_t* nnz);
+void lp_read(const std::string& path, LpArrays& out);
+
 // The CUDA engine (engine.cu). All functions throw Error.
 struct EngineImpl;
 EngineImpl* engine_create(const b2_lp_view& U, const b2_lp_view& S, const double* Dr, const double* Dc,
@@ -131,6 +144,7 @@ struct ServerImpl;
 ServerImpl* server_create(const b2_server_opts& so, const b2_solve_opts& o);
 void server_destroy(ServerImpl* s);
 int64_t server_submit(ServerImpl* s, const b2_lp_view& U);
+int64_t server_submit_file(ServerImpl* s, const std::string& path);
 int server_wait(ServerImpl* s, int64_t ticket, double timeout_s, double* x, double* y, b2_result* res,
                 b2_request_info* info);
 void server_stats(ServerImpl* s, b2_server_stats* out);

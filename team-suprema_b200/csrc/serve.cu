@@ -168,6 +168,7 @@ enum ReqState { RQ_SUBMITTED = 0, RQ_PREPARED = 1, RQ_RESIDENT = 2, RQ_DONE = 3 
 
 struct Request {
     int64_t ticket = 0;
+    std::string path;  // a request file, read on a preparation thread
     // the LP as submitted (unscaled PDLP form)
     int32_t m = 0, n = 0;
     std::vector<int32_t> row, col;
@@ -372,6 +373,16 @@ struct ServerImpl {
         r->rL.assign(U.rL, U.rL + U.m);
         r->rU.assign(U.rU, U.rU + U.m);
         r->obj_offset = U.obj_offset;
+        return enqueue(std::move(r));
+    }
+
+    int64_t submit_file(const std::string& path) {
+        std::unique_ptr<Request> r(new Request());
+        r->path = path;
+        return enqueue(std::move(r));
+    }
+
+    int64_t enqueue(std::unique_ptr<Request> r) {
         std::lock_guard<std::mutex> lk(mu);
         if (fatal) fail(fatal, "server stopped after an error: " + fatal_msg);
         if (stopping) fail(B2_ERR_INVALID, "server is shutting down");
@@ -420,6 +431,15 @@ struct ServerImpl {
     // Scaling (src/scaling.cpp:25-84, 10 Ruiz passes + Pock-Chambolle) and the
     // device layout; the batched lane also gets its region plan and image.
     void prepare(Request& r) {
+        if (!r.path.empty()) {
+            LpArrays a;
+            lp_read(r.path, a);
+            r.m = a.m;
+            r.n = a.n;
+            r.row.swap(a.row); r.col.swap(a.col); r.val.swap(a.val);
+            r.c.swap(a.c); r.l.swap(a.l); r.u.swap(a.u); r.rL.swap(a.rL); r.rU.swap(a.rU);
+            r.obj_offset = a.obj_offset;
+        }
         b2_lp_view U{r.m, r.n, (int64_t)r.val.size(), r.row.data(), r.col.data(), r.val.data(), r.c.data(),
                      r.rL.data(), r.rU.data(), r.l.data(), r.u.data(), r.obj_offset};
         std::vector<double> val_s(r.val.size()), c_s(r.n), l_s(r.n), u_s(r.n), rL_s(r.m), rU_s(r.m), Dr(r.m),
@@ -745,8 +765,12 @@ struct ServerImpl {
     void run_grid_slice() {
         Request* r = grid_resident.front();
         const auto t0 = Clock::now();
-        // short slices while batched LPs wait, long ones when the LP is alone
-        const double slice_ms = resident.empty() ? so.grid_slice_ms : std::min(so.grid_slice_ms, so.round_ms);
+        // short slices while the batched LPs could fill most of the GPU, long
+        // ones when the LP is alone or the rounds would leave most SMs idle
+        // (a round's CTAs: one per small LP, a cluster per large one)
+        int64_t need = 0;
+        for (const Request* q : resident) need += q->cluster && max_clusters > 0 ? dev::kMaxCluster : 1;
+        const double slice_ms = need * 2 < max_ctas ? so.grid_slice_ms : std::min(so.grid_slice_ms, so.round_ms);
         const bool ended = engine_slice(r->eng, o, slice_ms, cs);
         r->rounds++;
         {
@@ -820,6 +844,7 @@ ServerImpl* server_create(const b2_server_opts& so, const b2_solve_opts& o) {
 }
 void server_destroy(ServerImpl* s) { delete s; }
 int64_t server_submit(ServerImpl* s, const b2_lp_view& U) { return s->submit(U); }
+int64_t server_submit_file(ServerImpl* s, const std::string& path) { return s->submit_file(path); }
 int server_wait(ServerImpl* s, int64_t ticket, double timeout_s, double* x, double* y, b2_result* res,
                 b2_request_info* info) {
     return s->wait(ticket, timeout_s, x, y, res, info);

@@ -104,7 +104,7 @@ def test_batch_stop_flag():
 
 
 def test_cluster_path_certified():
-    """LPs above the cluster threshold are solved by a cluster of 8 CTAs
+    """LPs above the cluster threshold are solved by a cluster of 16 CTAs
     (hardware cluster barrier); answers are certified like the one-CTA path."""
     names, probs = fixture_problems()
     with B.Batch(probs) as bt:

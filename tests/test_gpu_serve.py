@@ -142,7 +142,7 @@ def test_malformed_request_fails_alone():
 
 @pytest.mark.parametrize("cluster_nnz", [1, 3000])
 def test_cluster_lane_equals_batched_cluster_path(cluster_nnz):
-    """Served LPs above cluster_nnz stored entries run on 8-CTA clusters (beside
+    """Served LPs above cluster_nnz stored entries run on 16-CTA clusters (beside
     a one-CTA launch for the rest); each answer is the batched engine's on the
     same path, bit for bit, however the rounds cut it."""
     names, probs = fixture_problems()
@@ -178,3 +178,43 @@ def test_pending_result_and_shutdown_with_requests_in_flight():
     with B.Server(round_ms=1.0) as s2:
         r, _ = s2.wait(s2.submit(U), timeout_s=60.0)
     certified(U, r, G["fixtures"]["afiro"]["simplex"]["objective"])
+
+
+def test_request_file_gives_the_same_answer(tmp_path):
+    """An LP submitted as a request file (read on the server's threads) is
+    solved exactly as the same LP submitted from memory; a bad path fails
+    its ticket alone."""
+    names, probs = fixture_problems()
+    U = B.RangedLP.like(probs[names.index("israel")][0])
+    path = str(tmp_path / "israel.b2lp")
+    B.write_lp(path, U)
+    with B.Server(round_ms=0.5) as srv:
+        a, _ = srv.wait(srv.submit(U), timeout_s=300.0)
+        b, _ = srv.wait(srv.submit_file(path), timeout_s=300.0)
+    # the file holds A row by row; the same LP, but its entries in another order
+    # may change the last bits, so the answers agree through the verifier
+    assert a.converged and b.converged
+    va = certified(U, a, G["fixtures"]["israel"]["simplex"]["objective"])
+    vb = certified(U, b, G["fixtures"]["israel"]["simplex"]["objective"])
+    assert rel(va["objective"], vb["objective"]) <= 1e-6
+    # the round-tripped LP in memory and the file: bit for bit
+    back = B.read_lp(path)
+    with B.Server(round_ms=0.5) as srv:
+        c, _ = srv.wait(srv.submit(back), timeout_s=300.0)
+    np.testing.assert_array_equal(c.x, b.x)
+    np.testing.assert_array_equal(c.y, b.y)
+    # a file whose header is sound but whose column index is out of range
+    import struct
+    blob = bytearray(open(path, "rb").read())
+    col0 = 32 + 8 * (U.m + 1)
+    blob[col0:col0 + 4] = struct.pack("<i", U.n + 9)
+    bad = str(tmp_path / "bad.b2lp")
+    open(bad, "wb").write(bytes(blob))
+    with B.Server(round_ms=0.5) as srv:
+        t_bad = srv.submit_file(bad)
+        t_ok = srv.submit(U)
+        with pytest.raises(B.B2Error) as e:
+            srv.wait(t_bad, timeout_s=60.0)
+        assert e.value.code == B.B2_ERR_INVALID
+        r, _ = srv.wait(t_ok, timeout_s=300.0)
+    np.testing.assert_array_equal(r.x, a.x)

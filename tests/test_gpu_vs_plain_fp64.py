@@ -85,3 +85,51 @@ def test_batch_vs_plain_fp64_gpu_one_at_a_time():
             "plain_ms_per_attempt": per_att * 1e3, "sample_lps": len(pick), "speedup": ours / plain}
     print("PLAIN_FP64_BATCH " + json.dumps(line))
     assert ours / plain >= 20.0, line
+
+
+def test_served_stream_vs_plain_fp64_fifo():
+    """The served mix (Poisson arrivals; 80 % m <= 2,000, 19 % up to 50,000,
+    1 % m = 500,000): a window of 53 requests, one of them m = 500,000, through
+    the server, against a FIFO server that solves them one at a time with the
+    plain FP64 engine. All arrive within 30 ms, so the FIFO makespan is the sum
+    of the plain engine's solve times; those are estimated per size class from
+    bounded runs of sampled requests (set-up + attempts x time per attempt,
+    with this engine's attempt counts)."""
+    import sys
+    from conftest import ROOT
+    sys.path.insert(0, ROOT)
+    import bench
+    stream = bench.serve_stream(2000.0, 0.03, 0)
+    lps = [B.gen_random_lp(m, n, k, sd, True) for (_, m, n, k, sd) in stream]
+    with B.Server(max_iterations=2_000_000, tol=1e-6) as srv:
+        ts = [srv.submit(lp) for lp in lps]
+        out = [srv.wait(t) for t in ts]
+    assert all(r.converged for r, _ in out)
+    first = min(info["submit_s"] for _, info in out)
+    last = max(info["done_s"] for _, info in out)
+    ours = len(out) / (last - first)
+    sizes = np.array([m for (_, m, *_r) in stream])
+    classes = {"small": sizes <= 2000, "mid": (sizes > 2000) & (sizes < 500_000), "large": sizes == 500_000}
+    plain_total = 0.0
+    detail = {}
+    for name, mask in classes.items():
+        idx = np.flatnonzero(mask)
+        if idx.size == 0:
+            continue
+        pick = idx[np.linspace(0, idx.size - 1, min(3, idx.size)).astype(int)]
+        setups, pers = [], []
+        for i in pick:
+            U = B.prepare(lps[i])[0]
+            P = O.RefProblem.from_form(as_form(U), use_presolve=False, gpu=True)
+            s, p = ref_time_model(P, 128, 640)
+            setups.append(s)
+            pers.append(p)
+        setup, per = float(np.mean(setups)), float(np.mean(pers))
+        t = sum(setup + out[i][0].iterations * per for i in idx)
+        plain_total += t
+        detail[name] = {"requests": int(idx.size), "plain_s": t, "plain_ms_per_attempt": per * 1e3}
+    plain = len(out) / plain_total
+    line = {"requests": len(out), "engine_solves_per_s": ours, "engine_makespan_s": last - first,
+            "plain_fp64_fifo_solves_per_s_est": plain, "classes": detail, "speedup": ours / plain}
+    print("PLAIN_FP64_SERVE " + json.dumps(line))
+    assert ours / plain >= 20.0, line
