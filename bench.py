@@ -55,14 +55,15 @@ REF_ATTEMPTS = {"large": 143360, "medium": 73024, "small": 13888}
 TRAFFIC_PER_ATTEMPT = {"large": (150.9e6, 203.9e6)}
 
 
-def describe(name):
+def describe(name, count=0, seconds=0.0, world=1):
     kind, p = WORKLOADS[name]
     if kind == "serve":
-        return (f"served stream: Poisson arrivals at {p['rate']:.0f} LPs/s for {p['seconds']} s; sizes 80% "
-                f"m~U[100,2000], 19% m~U[2000,50000], 1% m=500000; n=3m, 6 nnz/col, FP32 values, seed {p['seed']}")
+        return (f"served stream: Poisson arrivals at {p['rate'] * world:.0f} LPs/s for {seconds or p['seconds']} s; "
+                f"sizes 80% m~U[100,2000], 19% m~U[2000,50000], 1% m=500000; n=3m, 6 nnz/col, FP32 values, "
+                f"seed {p['seed']}")
     if kind == "batch":
-        return (f"batch of {p['count']} random equality LPs, m log-uniform [50,5000], n=round(U[2,4] m), "
-                f"U{{4..10}} nnz/col, FP32 values, seed {p['seed']}")
+        return (f"batch of {(count or p['count']) * world} random equality LPs, m log-uniform [50,5000], "
+                f"n=round(U[2,4] m), U{{4..10}} nnz/col, FP32 values, seed {p['seed']}")
     if kind == "random":
         return (f"random equality LP m={p['m']} n={p['n']} {p['k']} nnz/col values "
                 f"{'FP32' if p['fp32'] else 'FP64'} U[-1,1], 0<=x<=10, seed {p['seed']}")
@@ -169,6 +170,27 @@ def dist_max(x: float, world: int) -> float:
     return float(t.item())
 
 
+def dist_sum(x: float, world: int) -> float:
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([x], dtype=torch.float64, device=dev)
+    dist.all_reduce(t, op=dist.ReduceOp.SUM)
+    return float(t.item())
+
+
+def my_share(B, work, world, rank, online=False):
+    """Indices of this rank's share of a batch (online=False) or a stream in
+    arrival order (online=True): every rank computes the same plan from the
+    same loads (b2_shard_plan), so no collective is needed to decide it."""
+    if world == 1:
+        return list(range(len(work)))
+    plan = B.shard_plan(work, world, online=online)
+    return [i for i in range(len(work)) if plan[i] == rank]
+
+
 def job_rate(world: int, units_per_rank: float, max_ms: float) -> float:
     """Whole-job throughput of `world` replicas that each processed
     units_per_rank units, timed as the max over ranks (ms)."""
@@ -234,15 +256,24 @@ def workload_config(args, U, lp):
             "parallelism": f"replicas x{args.gpus}" if args.gpus > 1 else "single GPU"}
 
 
-def make_batch(B, name, count=0, m_hi=0):
+def batch_shapes(B, name, count=0, m_hi=0, world=1):
+    """The batch of `count` LPs per GPU: world x count shapes drawn from one
+    master seed (the single-GPU batch is the first draw of the same family)."""
     _, p = WORKLOADS[name]
+    return B.batch_family_shapes((count or p["count"]) * world, p["seed"], m_hi=m_hi or 5000)
+
+
+def make_batch(B, name, count=0, m_hi=0, world=1, rank=0):
+    """This rank's share of the batch (all of it on one GPU), balanced by load."""
+    shapes = batch_shapes(B, name, count, m_hi, world)
+    mine = my_share(B, [B.request_work(m, n, n * k) for (m, n, k, _) in shapes], world, rank)
     probs = []
-    shapes = B.batch_family_shapes(count or p["count"], p["seed"], m_hi=m_hi or 5000)
-    for (m, n, k, seed) in shapes:
+    for i in mine:
+        m, n, k, seed = shapes[i]
         lp = B.gen_random_lp(m, n, k, seed, True)
         U, S, Dr, Dc, _ = B.prepare(lp)
         probs.append((U, S, Dr, Dc))
-    return probs
+    return probs, len(shapes)
 
 
 def batch_bench(args, world, rank, local):
@@ -252,7 +283,7 @@ def batch_bench(args, world, rank, local):
     torch.cuda.set_device(local)
     prec = B.PREC_MIXED if args.precision == "mixed" else B.PREC_FP64
     t0 = time.time()
-    probs = make_batch(B, args.workload, args.batch_count, args.batch_mhi)
+    probs, n_total = make_batch(B, args.workload, args.batch_count, args.batch_mhi, world, rank)
     t_prep = time.time() - t0
     t0 = time.time()
     bt = B.Batch(probs)
@@ -270,10 +301,11 @@ def batch_bench(args, world, rank, local):
     dist_barrier(world)
     ms_total = dist_max(sum(ms for _, ms in steps), world)
     n_lp = len(probs)
-    value = job_rate(world, n_lp * args.steps, ms_total)
+    # every rank solves its own share: the job's throughput is all LPs over the slowest rank
+    value = n_total * args.steps / (ms_total / 1e3)
     res = steps[-1][0]
     lat = sorted(r["device_ms"] for r in res)
-    conv = sum(r["converged"] for r in res)
+    conv = int(dist_sum(sum(r["converged"] for r in res), world))
     attempts = np.array([r["iterations"] for r in res])
     if rank == 0:
         line = {
@@ -281,13 +313,15 @@ def batch_bench(args, world, rank, local):
             "warmup": args.warmup, "ms_per_step": ms_total / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64" if prec == B.PREC_MIXED else "f64",
             "data": "synthetic",
-            "config": {"workload": describe(args.workload), "lps": n_lp, "m_hi": args.batch_mhi or 5000,
-                       "sum_m": info["sum_m"],
-                       "sum_n": info["sum_n"], "sum_nnz": info["sum_nnz"], "tol": args.tol,
+            "config": {"workload": describe(args.workload, count=args.batch_count, world=world), "lps": n_total,
+                       "lps_rank0": n_lp,
+                       "m_hi": args.batch_mhi or 5000, "sum_m_rank0": info["sum_m"],
+                       "sum_n_rank0": info["sum_n"], "sum_nnz_rank0": info["sum_nnz"], "tol": args.tol,
                        "batch_block": bt.info()["threads_per_cta"], "batch_cluster_nnz": args.batch_cluster_nnz,
-                       "parallelism": f"replicas x{world}" if world > 1 else "single GPU"},
+                       "parallelism": f"sharded x{world} (load-balanced shares, no collective)" if world > 1
+                       else "single GPU"},
             "latency_ms": {"p50": lat[len(lat) // 2], "p99": lat[int(0.99 * (len(lat) - 1))], "max": lat[-1],
-                           "note": "per-LP time on its CTA inside the launch"},
+                           "note": "per-LP time on its CTA inside the launch (rank 0's share)"},
             "converged": conv, "attempts": {"median": float(np.median(attempts)), "max": int(attempts.max()),
                                             "total": int(attempts.sum())},
             "clocks": clk.summary(), "gpu_launches": args.steps, "prep_s": t_prep, "create_s": t_create,
@@ -323,7 +357,11 @@ def serve_bench(args, world, rank, local):
     torch.cuda.set_device(local)
     prec = B.PREC_MIXED if args.precision == "mixed" else B.PREC_FP64
     _, p = WORKLOADS[args.workload]
-    stream = serve_stream(p["rate"], args.serve_seconds or p["seconds"], p["seed"])
+    # the offered rate grows with the GPUs (weak scaling); each rank serves its
+    # share of the one stream, routed in arrival order to the least-loaded rank
+    full = serve_stream(p["rate"] * world, args.serve_seconds or p["seconds"], p["seed"])
+    mine = my_share(B, [B.request_work(m, n, n * k) for (_, m, n, k, _) in full], world, rank, online=True)
+    stream = [full[i] for i in mine]
     t0 = time.time()
     lps = [B.gen_random_lp(m, n, k, sd, True) for (_, m, n, k, sd) in stream]
     t_gen = time.time() - t0
@@ -347,28 +385,38 @@ def serve_bench(args, world, rank, local):
         st1 = srv.stats()
     dist_barrier(world)
     lat = np.array([(info["done_s"] - info["submit_s"]) * 1e3 for _, info in out])
-    first = min(info["submit_s"] for _, info in out)
-    last = max(info["done_s"] for _, info in out)
-    makespan = dist_max(last - first, world)
-    value = job_rate(world, len(out), makespan * 1e3)
-    conv = sum(r.converged for r, _ in out)
-    worst = max(max(r.eps_P, r.eps_D, r.eps_G) for r, _ in out)
+    # from the stream's first arrival to the last answer on any rank (the ranks
+    # start their arrival clocks together, after the barrier)
+    end = 0.0
+    if out:
+        first = min(info["submit_s"] for _, info in out)
+        last = max(info["done_s"] for _, info in out)
+        end = last - first + stream[0][0]
+    makespan = dist_max(end, world) - full[0][0]
+    value = len(full) / makespan
+    conv = int(dist_sum(sum(r.converged for r, _ in out), world))
+    worst = dist_max(max((max(r.eps_P, r.eps_D, r.eps_G) for r, _ in out), default=0.0), world)
     lanes = [info["lane"] for _, info in out]
     sizes = np.array([m for (_, m, *_rest) in stream])
+    sizes_all = np.array([m for (_, m, *_rest) in full])
     if rank == 0:
         q = lambda a, f: float(np.quantile(a, f)) if len(a) else None  # noqa: E731
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": 1, "warmup": args.warmup,
             "ms_per_step": makespan * 1e3, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f32+f64" if prec == B.PREC_MIXED else "f64", "data": "synthetic",
-            "config": {"workload": describe(args.workload), "requests": len(out),
-                       "offered_per_s": len(out) / (args.serve_seconds or p["seconds"]),
-                       "classes": {"m<=2000": int((sizes <= 2000).sum()),
-                                   "2000<m<=50000": int(((sizes > 2000) & (sizes <= 50000)).sum()),
-                                   "m=500000": int((sizes == 500_000).sum())},
+            "config": {"workload": describe(args.workload, seconds=args.serve_seconds, world=world),
+                       "requests": len(full), "requests_rank0": len(out),
+                       "offered_per_s": len(full) / (args.serve_seconds or p["seconds"]),
+                       "classes": {"m<=2000": int((sizes_all <= 2000).sum()),
+                                   "2000<m<=50000": int(((sizes_all > 2000) & (sizes_all <= 50000)).sum()),
+                                   "m=500000": int((sizes_all == 500_000).sum())},
                        "tol": args.tol, "round_ms": args.round_ms, "hbm_budget_gb": 150,
-                       "parallelism": f"replicas x{world}" if world > 1 else "single GPU"},
-            "latency_ms": {"p50": q(lat, 0.5), "p99": q(lat, 0.99), "p999": q(lat, 0.999), "max": float(lat.max()),
+                       "parallelism": f"sharded x{world} (requests routed in arrival order to the least-loaded "
+                                      "rank, no collective)" if world > 1 else "single GPU"},
+            "latency_ms": {"p50": q(lat, 0.5), "p99": q(lat, 0.99), "p999": q(lat, 0.999),
+                           "max": float(lat.max()) if len(lat) else None,
+                           "of": "rank 0's requests" if world > 1 else "all requests",
                            "p50_small": q(lat[sizes <= 2000], 0.5), "p99_small": q(lat[sizes <= 2000], 0.99)},
             "converged": int(conv), "worst_kkt": worst, "whole_gpu_lane": int(sum(lanes)),
             "server": {"rounds": st1["rounds"] - st0["rounds"], "grid_slices": st1["grid_slices"] - st0["grid_slices"],

@@ -258,6 +258,7 @@ typedef struct b2_server_stats {
     int32_t resident, queued;
     int64_t bytes_in_use, peak_bytes;
     double busy_ms;                   /* device time of rounds and slices                    */
+    int64_t backlog_work;             /* sum of b2_request_work() over requests not finished  */
 } b2_server_stats;
 
 /* opts: solve options for every request (tol, precision, max_iterations, ...);
@@ -280,6 +281,43 @@ int b2_server_stats_get(b2_server* s, b2_server_stats* out);
 /* Stops the server: running LPs stop at their next poll, unclaimed results are
  * dropped. No other call on this server may be in progress or follow. */
 void b2_server_destroy(b2_server* s);
+
+/* ---- several GPUs: shares of a batch or a stream -------------------------
+ * No counterpart in the reference (one LP, one device). LPs are independent,
+ * so a batch or a stream spreads over GPUs with no exchange between them:
+ * each GPU solves its own share, one process per GPU (b2_shard_plan) or one
+ * process driving a server per GPU (b2_pool). The unit of load is
+ * b2_request_work(m, n, nnz) = 2 nnz + m + n, the matrix entries and vector
+ * elements one PDHG attempt passes over (both products, both vector passes). */
+int64_t b2_request_work(int32_t m, int32_t n, int64_t nnz);
+
+/* Assigns `count` items of load work[i] >= 0 to `parts` shares; rank_of[i]
+ * receives item i's share. online = 0 (a batch known up front): items by
+ * decreasing load (equal loads by index), each to the least-loaded share
+ * (longest-processing-time first). online = 1 (a stream): items in the given
+ * order, each to the share with the least load so far. Equal shares go to the
+ * lower index. Deterministic: every rank computes the same plan from the same
+ * list, so ranks agree on their shares without a collective. */
+int b2_shard_plan(const int64_t* work, int64_t count, int32_t parts, int32_t online, int32_t* rank_of);
+
+/* A pool of servers, one per listed device, in one process. Each submit goes
+ * to the member with the least unfinished work (b2_server_stats.backlog_work;
+ * equal backlogs to the lower member), so work finished on a fast GPU frees it
+ * for the next request. Each LP is solved exactly as by a single server, so
+ * its answer does not depend on which member took it. Tickets are the pool's
+ * own. devices may repeat (several servers on one GPU). */
+typedef struct b2_pool b2_pool;
+
+int b2_pool_create(const int32_t* devices, int32_t count, const b2_server_opts* sopts, const b2_solve_opts* opts,
+                   b2_pool** out);
+int b2_pool_submit(b2_pool* p, const b2_lp_view* unscaled_form, int64_t* ticket);
+int b2_pool_submit_file(b2_pool* p, const char* path, int64_t* ticket);
+/* As b2_server_wait; member (may be NULL) receives the index (into the create
+ * call's device list) of the server that solved the request. */
+int b2_pool_wait(b2_pool* p, int64_t ticket, double timeout_s, double* x, double* y, b2_result* res,
+                 b2_request_info* info, int32_t* member);
+int b2_pool_stats_get(b2_pool* p, int32_t member, b2_server_stats* out);
+void b2_pool_destroy(b2_pool* p);
 
 /* ---- host-side preparation (product side, no GPU needed) ---------------- */
 

@@ -44,6 +44,8 @@ EXPORTED = [
     "b2_batch_destroy",
     "b2_server_create", "b2_server_submit", "b2_server_submit_file", "b2_server_wait", "b2_server_stats_get",
     "b2_server_destroy", "b2_lp_write", "b2_lp_read_dims", "b2_lp_read",
+    "b2_request_work", "b2_shard_plan", "b2_pool_create", "b2_pool_submit", "b2_pool_submit_file",
+    "b2_pool_wait", "b2_pool_stats_get", "b2_pool_destroy",
     "b2_scale", "b2_scale_gpu",
     "b2_gen_random_lp", "b2_gen_transport", "b2_last_error", "b2_version",
 ]
@@ -102,7 +104,7 @@ class ServerStats(C.Structure):
     _fields_ = [("submitted", C.c_int64), ("completed", C.c_int64), ("failed", C.c_int64),
                 ("rounds", C.c_int64), ("grid_slices", C.c_int64), ("resident", C.c_int32),
                 ("queued", C.c_int32), ("bytes_in_use", C.c_int64), ("peak_bytes", C.c_int64),
-                ("busy_ms", C.c_double)]
+                ("busy_ms", C.c_double), ("backlog_work", C.c_int64)]
 
 
 class EngineInfo(C.Structure):
@@ -160,6 +162,16 @@ def lib():
             L.b2_server_wait.argtypes = [vp, i64, f64, vp, vp, C.POINTER(_Result), C.POINTER(RequestInfo)]
             L.b2_server_stats_get.argtypes = [vp, C.POINTER(ServerStats)]
             L.b2_server_destroy.argtypes = [vp]
+            L.b2_request_work.argtypes = [i32, i32, i64]
+            L.b2_request_work.restype = i64
+            L.b2_shard_plan.argtypes = [vp, i64, i32, i32, vp]
+            L.b2_pool_create.argtypes = [vp, i32, C.POINTER(ServerOpts), C.POINTER(SolveOpts), C.POINTER(vp)]
+            L.b2_pool_submit.argtypes = [vp, C.POINTER(_LPView), C.POINTER(i64)]
+            L.b2_pool_submit_file.argtypes = [vp, C.c_char_p, C.POINTER(i64)]
+            L.b2_pool_wait.argtypes = [vp, i64, f64, vp, vp, C.POINTER(_Result), C.POINTER(RequestInfo),
+                                       C.POINTER(i32)]
+            L.b2_pool_stats_get.argtypes = [vp, i32, C.POINTER(ServerStats)]
+            L.b2_pool_destroy.argtypes = [vp]
             L.b2_server_destroy.restype = None
             L.b2_scale.argtypes = [C.POINTER(_LPView), i32] + [vp] * 8
             L.b2_scale_gpu.argtypes = [C.POINTER(_LPView), i32] + [vp] * 8
@@ -530,6 +542,84 @@ class Server:
     def stats(self) -> dict:
         st = ServerStats()
         _check(lib().b2_server_stats_get(self._h, C.byref(st)))
+        return {k: getattr(st, k) for k, _ in ServerStats._fields_}
+
+
+# --------------------------------------------------- shares over several GPUs
+def request_work(m: int, n: int, nnz: int) -> int:
+    """The load unit of sharding and routing: 2 nnz + m + n (b2_request_work)."""
+    return int(lib().b2_request_work(int(m), int(n), int(nnz)))
+
+
+def shard_plan(work, parts: int, online: bool = False) -> np.ndarray:
+    """Share index of every item (b2_shard_plan): online=False, longest load
+    first to the least-loaded share (a batch); online=True, in the given order
+    to the least-loaded share so far (a stream). Every rank computes the same
+    plan from the same list, so no collective is needed."""
+    w = np.ascontiguousarray(work, dtype=np.int64)
+    out = np.zeros(max(w.size, 1), np.int32)
+    _check(lib().b2_shard_plan(_ptr(w), int(w.size), int(parts), int(bool(online)), _ptr(out)))
+    return out[:w.size]
+
+
+class Pool(Server):
+    """One server per listed device in this process (b2_pool_*); each submit
+    goes to the member with the least unfinished work. wait(ticket) returns
+    (PdlpResult, info) with info["member"] the index of the server that
+    solved it; stats(member) that member's counters."""
+
+    def __init__(self, devices=(0,), hbm_budget_bytes: float = 0.0, round_ms: float = 0.0, max_resident: int = 0,
+                 prep_threads: int = 0, grid_nnz: int = 0, grid_slice_ms: float = 0.0, cluster_nnz: int = 0,
+                 gpu_scale_nnz: int = 0, **opts):
+        so = ServerOpts(float(hbm_budget_bytes), float(round_ms), int(max_resident), int(prep_threads),
+                        int(grid_nnz), float(grid_slice_ms), int(cluster_nnz), int(gpu_scale_nnz))
+        o = default_opts(**opts)
+        dv = np.ascontiguousarray(list(devices), dtype=np.int32)
+        h = C.c_void_p()
+        _check(lib().b2_pool_create(_ptr(dv), int(dv.size), C.byref(so), C.byref(o), C.byref(h)))
+        self._h = h
+        self._dims = {}
+        self.members = int(dv.size)
+
+    def close(self):
+        if getattr(self, "_h", None) and self._h.value:
+            lib().b2_pool_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def submit(self, unscaled_form: RangedLP) -> int:
+        U = RangedLP.like(unscaled_form)
+        t = C.c_int64()
+        _check(lib().b2_pool_submit(self._h, C.byref(U.view()), C.byref(t)))
+        self._dims[t.value] = (U.m, U.n)
+        return t.value
+
+    def submit_file(self, path: str) -> int:
+        m, n, _ = lp_file_dims(path)
+        t = C.c_int64()
+        _check(lib().b2_pool_submit_file(self._h, os.fsencode(path), C.byref(t)))
+        self._dims[t.value] = (m, n)
+        return t.value
+
+    def wait(self, ticket: int, timeout_s: float = -1.0):
+        m, n = self._dims[ticket]
+        x = np.zeros(max(n, 1))
+        y = np.zeros(max(m, 1))
+        r = _Result()
+        inf = RequestInfo()
+        k = C.c_int32(-1)
+        rc = lib().b2_pool_wait(self._h, int(ticket), float(timeout_s), _ptr(x), _ptr(y), C.byref(r), C.byref(inf),
+                                C.byref(k))
+        if rc == B2_ERR_PENDING:
+            return None
+        del self._dims[ticket]
+        _check(rc)
+        info = {k_: getattr(inf, k_) for k_, _ in RequestInfo._fields_}
+        info["member"] = k.value
+        return _result(r, x[:n], y[:m]), info
+
+    def stats(self, member: int = 0) -> dict:
+        st = ServerStats()
+        _check(lib().b2_pool_stats_get(self._h, int(member), C.byref(st)))
         return {k: getattr(st, k) for k, _ in ServerStats._fields_}
 
 

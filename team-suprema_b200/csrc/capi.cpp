@@ -55,6 +55,10 @@ struct b2_server {
     b2::ServerImpl* impl;
 };
 
+struct b2_pool {
+    b2::PoolImpl* impl;
+};
+
 extern "C" {
 
 void b2_default_opts(b2_solve_opts* o) {
@@ -250,6 +254,67 @@ void b2_server_destroy(b2_server* s) {
     if (!s) return;
     b2::server_destroy(s->impl);
     delete s;
+}
+
+int64_t b2_request_work(int32_t m, int32_t n, int64_t nnz) { return b2::request_work(m, n, nnz); }
+
+int b2_shard_plan(const int64_t* work, int64_t count, int32_t parts, int32_t online, int32_t* rank_of) {
+    return b2::guarded([&] { b2::shard_plan(work, count, parts, online != 0, rank_of); });
+}
+
+int b2_pool_create(const int32_t* devices, int32_t count, const b2_server_opts* sopts, const b2_solve_opts* opts,
+                   b2_pool** out) {
+    return b2::guarded([&] {
+        if (!out) b2::fail(B2_ERR_INVALID, "null argument");
+        *out = nullptr;
+        b2_server_opts so;
+        std::memset(&so, 0, sizeof(so));
+        if (sopts) so = *sopts;
+        b2_solve_opts o;
+        if (opts) o = *opts;
+        else b2_default_opts(&o);
+        b2::PoolImpl* p = b2::pool_create(devices, count, so, o);
+        *out = new b2_pool{p};
+    });
+}
+
+int b2_pool_submit(b2_pool* p, const b2_lp_view* U, int64_t* ticket) {
+    return b2::guarded([&] {
+        if (!p || !U || !ticket) b2::fail(B2_ERR_INVALID, "null argument");
+        *ticket = b2::pool_submit(p->impl, *U);
+    });
+}
+
+int b2_pool_submit_file(b2_pool* p, const char* path, int64_t* ticket) {
+    return b2::guarded([&] {
+        if (!p || !path || !ticket) b2::fail(B2_ERR_INVALID, "null argument");
+        *ticket = b2::pool_submit_file(p->impl, path);
+    });
+}
+
+int b2_pool_wait(b2_pool* p, int64_t ticket, double timeout_s, double* x, double* y, b2_result* res,
+                 b2_request_info* info, int32_t* member) {
+    int rc = B2_OK;
+    const int g = b2::guarded([&] {
+        if (!p) b2::fail(B2_ERR_INVALID, "null argument");
+        rc = b2::pool_wait(p->impl, ticket, timeout_s, x, y, res, info, member);
+    });
+    if (g != B2_OK) return g;
+    if (rc == B2_ERR_PENDING) b2::set_last_error("request not finished yet");
+    return rc;
+}
+
+int b2_pool_stats_get(b2_pool* p, int32_t member, b2_server_stats* out) {
+    return b2::guarded([&] {
+        if (!p || !out) b2::fail(B2_ERR_INVALID, "null argument");
+        b2::pool_stats(p->impl, member, out);
+    });
+}
+
+void b2_pool_destroy(b2_pool* p) {
+    if (!p) return;
+    b2::pool_destroy(p->impl);
+    delete p;
 }
 
 int b2_batch_create(int32_t n_lp, const b2_lp_view* U, const b2_lp_view* S, const double* const* Dr,

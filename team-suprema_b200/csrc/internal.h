@@ -148,5 +148,18 @@ int64_t server_submit_file(ServerImpl* s, const std::string& path);
 int server_wait(ServerImpl* s, int64_t ticket, double timeout_s, double* x, double* y, b2_result* res,
                 b2_request_info* info);
 void server_stats(ServerImpl* s, b2_server_stats* out);
+int64_t server_backlog(ServerImpl* s);  // b2_server_stats.backlog_work
+
+// Shares over several GPUs (pool.cpp). All functions throw Error.
+int64_t request_work(int32_t m, int32_t n, int64_t nnz);
+void shard_plan(const int64_t* work, int64_t count, int32_t parts, bool online, int32_t* rank_of);
+struct PoolImpl;
+PoolImpl* pool_create(const int32_t* devices, int32_t count, const b2_server_opts& so, const b2_solve_opts& o);
+void pool_destroy(PoolImpl* p);
+int64_t pool_submit(PoolImpl* p, const b2_lp_view& U);
+int64_t pool_submit_file(PoolImpl* p, const std::string& path);
+int pool_wait(PoolImpl* p, int64_t ticket, double timeout_s, double* x, double* y, b2_result* res,
+              b2_request_info* info, int32_t* member);
+void pool_stats(PoolImpl* p, int32_t member, b2_server_stats* out);
 
 }  // namespace b2

@@ -196,6 +196,7 @@ struct Request {
     double t_submit = 0, t_prepared = 0, t_admit = 0, t_done = 0, prep_ms = 0;
     int rounds = 0;
     int qpos = -1;
+    int64_t work = 0;  // request_work() of the LP, counted in the server's backlog until done
 };
 
 // Pinned staging for the copies out of finished LPs, so that one round's
@@ -341,6 +342,10 @@ struct ServerImpl {
         cv_loop.notify_all();
         for (auto& t : preppers) t.join();
         if (loop.joinable()) loop.join();
+        // the caller may have another device current (a pool of servers)
+        int caller = -1;
+        if (cudaGetDevice(&caller) != cudaSuccess) caller = -1;
+        if (cs) cudaSetDevice(device);
         if (cs) cudaStreamSynchronize(cs);
         if (ds) cudaStreamSynchronize(ds);
         for (auto& kv : reqs) release(kv.second), delete kv.second;
@@ -354,6 +359,7 @@ struct ServerImpl {
         if (cs2) cudaStreamDestroy(cs2);
         if (cs) cudaStreamDestroy(cs);
         if (ds) cudaStreamDestroy(ds);
+        if (caller >= 0) cudaSetDevice(caller);
     }
 
     // ---- submission and preparation ----
@@ -373,12 +379,23 @@ struct ServerImpl {
         r->rL.assign(U.rL, U.rL + U.m);
         r->rU.assign(U.rU, U.rU + U.m);
         r->obj_offset = U.obj_offset;
+        r->work = request_work(U.m, U.n, U.nnz);
         return enqueue(std::move(r));
     }
 
     int64_t submit_file(const std::string& path) {
         std::unique_ptr<Request> r(new Request());
         r->path = path;
+        // the header alone sizes the backlog; a file that cannot be read
+        // counts nothing and fails its ticket on a preparation thread
+        try {
+            int32_t m = 0, n = 0;
+            int64_t nnz = 0;
+            lp_read_dims(path, &m, &n, &nnz);
+            r->work = request_work(m, n, nnz);
+        } catch (const Error&) {
+            r->work = 0;
+        }
         return enqueue(std::move(r));
     }
 
@@ -392,6 +409,7 @@ struct ServerImpl {
         reqs[p->ticket] = p;
         prep_q.push_back(p);
         st.submitted++;
+        st.backlog_work += p->work;
         cv_prep.notify_one();
         return p->ticket;
     }
@@ -488,6 +506,7 @@ struct ServerImpl {
             r->err = code ? code : B2_ERR_INVALID;
             r->err_msg = msg;
             r->state = RQ_DONE;
+            st.backlog_work -= r->work;
             r->t_done = now_s();
             st.failed++;
         }
@@ -603,6 +622,7 @@ struct ServerImpl {
                 r->err = e.code;
                 r->err_msg = e.msg;
                 r->state = RQ_DONE;
+                st.backlog_work -= r->work;
                 r->t_done = now_s();
                 st.failed++;
                 cv_done.notify_all();
@@ -741,6 +761,7 @@ struct ServerImpl {
                     // the caller may take (and delete) it once it is marked done
                     release(r);
                     r->state = RQ_DONE;
+                    st.backlog_work -= r->work;
                     r->t_done = t;
                     st.completed++;
                 } else {
@@ -788,6 +809,7 @@ struct ServerImpl {
             grid_resident.pop_front();
             release(r);
             r->state = RQ_DONE;
+            st.backlog_work -= r->work;
             r->t_done = now_s();
             st.completed++;
         }
@@ -850,5 +872,9 @@ int server_wait(ServerImpl* s, int64_t ticket, double timeout_s, double* x, doub
     return s->wait(ticket, timeout_s, x, y, res, info);
 }
 void server_stats(ServerImpl* s, b2_server_stats* out) { s->stats(out); }
+int64_t server_backlog(ServerImpl* s) {
+    std::lock_guard<std::mutex> lk(s->mu);
+    return s->st.backlog_work;
+}
 
 }  // namespace b2
