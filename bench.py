@@ -441,8 +441,9 @@ def profile_mode(args):
             print(f"spmv A {a * 1e3:.1f} us, A^T {t * 1e3:.1f} us ({args.precision} vectors)")
         else:
             r = eng.solve(max_iterations=args.max_attempts, tol=args.tol, precision=prec, copy_out=False)
-            print(f"solve: {r.iterations} attempts, {r.stats['device_ms']:.2f} ms, "
-                  f"{1e3 * r.stats['device_ms'] / max(1, r.iterations):.1f} us/attempt")
+            print(f"solve: {r.iterations} attempts ({r.stats['fp32_attempts']} FP32), "
+                  f"{r.stats['device_ms']:.2f} ms, {1e3 * r.stats['device_ms'] / max(1, r.iterations):.1f} us/attempt, "
+                  f"tol {args.tol:g}, converged {r.converged}, eps {r.eps_P:.3e} {r.eps_D:.3e} {r.eps_G:.3e}")
 
 
 def main():
