@@ -319,6 +319,14 @@ int b2_pool_wait(b2_pool* p, int64_t ticket, double timeout_s, double* x, double
 int b2_pool_stats_get(b2_pool* p, int32_t member, b2_server_stats* out);
 void b2_pool_destroy(b2_pool* p);
 
+/* Builds the device layout of an LP on the host (no GPU) exactly as
+ * b2_engine_create (whole_gpu = 1: long rows tuned and split) or a batch /
+ * server LP (whole_gpu = 0) does, with `threads` host threads, and returns a
+ * 64-bit digest of every byte the device would receive. The layout does not
+ * depend on the thread count; this is how that is checked. */
+int b2_layout_digest(const b2_lp_view* unscaled_form, const b2_lp_view* scaled_form, const double* Dr,
+                     const double* Dc, int32_t threads, int32_t whole_gpu, uint64_t* digest);
+
 /* ---- host-side preparation (product side, no GPU needed) ---------------- */
 
 /* Ruiz (ruiz_passes) + Pock-Chambolle alpha=1 scaling, as scale() in

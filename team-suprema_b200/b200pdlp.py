@@ -44,7 +44,7 @@ EXPORTED = [
     "b2_batch_destroy",
     "b2_server_create", "b2_server_submit", "b2_server_submit_file", "b2_server_wait", "b2_server_stats_get",
     "b2_server_destroy", "b2_lp_write", "b2_lp_read_dims", "b2_lp_read",
-    "b2_request_work", "b2_shard_plan", "b2_pool_create", "b2_pool_submit", "b2_pool_submit_file",
+    "b2_layout_digest", "b2_request_work", "b2_shard_plan", "b2_pool_create", "b2_pool_submit", "b2_pool_submit_file",
     "b2_pool_wait", "b2_pool_stats_get", "b2_pool_destroy",
     "b2_scale", "b2_scale_gpu",
     "b2_gen_random_lp", "b2_gen_transport", "b2_last_error", "b2_version",
@@ -162,6 +162,8 @@ def lib():
             L.b2_server_wait.argtypes = [vp, i64, f64, vp, vp, C.POINTER(_Result), C.POINTER(RequestInfo)]
             L.b2_server_stats_get.argtypes = [vp, C.POINTER(ServerStats)]
             L.b2_server_destroy.argtypes = [vp]
+            L.b2_layout_digest.argtypes = [C.POINTER(_LPView), C.POINTER(_LPView), vp, vp, i32, i32,
+                                           C.POINTER(C.c_uint64)]
             L.b2_request_work.argtypes = [i32, i32, i64]
             L.b2_request_work.restype = i64
             L.b2_shard_plan.argtypes = [vp, i64, i32, i32, vp]
@@ -543,6 +545,21 @@ class Server:
         st = ServerStats()
         _check(lib().b2_server_stats_get(self._h, C.byref(st)))
         return {k: getattr(st, k) for k, _ in ServerStats._fields_}
+
+
+def layout_digest(unscaled_form: RangedLP, scaled_form: RangedLP, Dr, Dc, threads: int = 1,
+                  whole_gpu: bool = True) -> int:
+    """64-bit digest of the device layout built on the host with `threads`
+    threads (b2_layout_digest): the one-LP engine's (whole_gpu) or a batched
+    LP's. Needs no GPU."""
+    U = RangedLP.like(unscaled_form)
+    S = RangedLP.like(scaled_form)
+    dr = _vec(Dr, U.m)
+    dc = _vec(Dc, U.n)
+    d = C.c_uint64()
+    _check(lib().b2_layout_digest(C.byref(U.view()), C.byref(S.view()), _ptr(dr), _ptr(dc), int(threads),
+                                  int(bool(whole_gpu)), C.byref(d)))
+    return d.value
 
 
 # --------------------------------------------------- shares over several GPUs

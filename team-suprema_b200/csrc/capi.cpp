@@ -256,6 +256,19 @@ void b2_server_destroy(b2_server* s) {
     delete s;
 }
 
+int b2_layout_digest(const b2_lp_view* U, const b2_lp_view* S, const double* Dr, const double* Dc, int32_t threads,
+                     int32_t whole_gpu, uint64_t* digest) {
+    return b2::guarded([&] {
+        if (!U || !S || !digest) b2::fail(B2_ERR_INVALID, "null argument");
+        b2::BuildParams bp;
+        bp.split = whole_gpu != 0;
+        bp.threads = threads > 0 ? threads : 1;
+        b2::Layout L;
+        b2::build_layout(*U, *S, Dr, Dc, bp, L);
+        *digest = b2::layout_digest(L);
+    });
+}
+
 int64_t b2_request_work(int32_t m, int32_t n, int64_t nnz) { return b2::request_work(m, n, nnz); }
 
 int b2_shard_plan(const int64_t* work, int64_t count, int32_t parts, int32_t online, int32_t* rank_of) {

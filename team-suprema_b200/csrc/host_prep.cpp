@@ -21,36 +21,123 @@ namespace {
 
 constexpr double kInf = std::numeric_limits<double>::infinity();
 
+// Runs f(begin, end, chunk) over [0, n) cut into contiguous chunks, one per
+// thread (at most `threads`, none shorter than `grain`); the calling thread
+// takes chunk 0. Returns the number of chunks.
+template <class F>
+int parallel_chunks(int threads, int64_t n, int64_t grain, F&& f) {
+    const int nch = (int)std::max<int64_t>(1, std::min<int64_t>(std::max(1, threads), n / std::max<int64_t>(1, grain)));
+    if (nch <= 1) {
+        f(int64_t(0), n, 0);
+        return 1;
+    }
+    const int64_t per = (n + nch - 1) / nch;
+    std::vector<std::thread> pool;
+    for (int t = 1; t < nch; ++t) {
+        const int64_t b = std::min(n, t * per), e = std::min(n, b + per);
+        pool.emplace_back([&f, b, e, t] { f(b, e, t); });
+    }
+    f(int64_t(0), std::min(n, per), 0);
+    for (auto& th : pool) th.join();
+    return nch;
+}
+
+// Smallest k in [0, n) with bad(k), or -1; chunks searched in parallel.
+template <class P>
+int64_t first_bad(int threads, int64_t n, P&& bad) {
+    std::vector<int64_t> hit((size_t)std::max(1, threads), -1);
+    parallel_chunks(threads, n, 1 << 16, [&](int64_t b, int64_t e, int t) {
+        for (int64_t k = b; k < e; ++k)
+            if (bad(k)) {
+                hit[t] = k;
+                return;
+            }
+    });
+    for (int64_t h : hit)
+        if (h >= 0) return h;  // chunks are in index order
+    return -1;
+}
+
 // CSR with the stable fill order of include/sparse.hpp:24-40 (entries of a row
-// keep their COO order).
+// keep their COO order). With several threads, each takes a contiguous run of
+// the COO entries: it counts its entries per row, the counts are turned into
+// per-run start offsets (earlier runs first inside every row), and each run
+// scatters its own entries, so the result is the serial one.
 void coo_to_csr(int64_t rows, int64_t nnz, const int32_t* r, const int32_t* c, const double* v,
-                std::vector<int64_t>& ptr, std::vector<int32_t>& idx, std::vector<double>& val) {
+                std::vector<int64_t>& ptr, std::vector<int32_t>& idx, std::vector<double>& val, int threads = 1) {
     ptr.assign(rows + 1, 0);
-    for (int64_t k = 0; k < nnz; ++k) ptr[r[k] + 1]++;
-    for (int64_t i = 0; i < rows; ++i) ptr[i + 1] += ptr[i];
     idx.resize(nnz);
     val.resize(nnz);
-    std::vector<int64_t> cur(ptr.begin(), ptr.end() - 1);
-    for (int64_t k = 0; k < nnz; ++k) {
-        int64_t p = cur[r[k]]++;
-        idx[p] = c[k];
-        val[p] = v[k];
+    const int nch = (int)std::max<int64_t>(1, std::min<int64_t>(std::max(1, threads), nnz / (1 << 18)));
+    if (nch <= 1) {
+        for (int64_t k = 0; k < nnz; ++k) ptr[r[k] + 1]++;
+        for (int64_t i = 0; i < rows; ++i) ptr[i + 1] += ptr[i];
+        std::vector<int64_t> cur(ptr.begin(), ptr.end() - 1);
+        for (int64_t k = 0; k < nnz; ++k) {
+            int64_t p = cur[r[k]]++;
+            idx[p] = c[k];
+            val[p] = v[k];
+        }
+        return;
     }
+    const int64_t per = (nnz + nch - 1) / nch;
+    std::vector<std::vector<int64_t>> cur((size_t)nch);
+    auto runs = [&](auto&& body) {
+        std::vector<std::thread> pool;
+        for (int t = 1; t < nch; ++t) pool.emplace_back([&body, t] { body(t); });
+        body(0);
+        for (auto& th : pool) th.join();
+    };
+    runs([&](int t) {
+        cur[t].assign((size_t)rows, 0);
+        const int64_t b = std::min(nnz, t * per), e = std::min(nnz, b + per);
+        for (int64_t k = b; k < e; ++k) cur[t][r[k]]++;
+    });
+    parallel_chunks(nch, rows, 1 << 14, [&](int64_t b, int64_t e, int) {
+        for (int64_t i = b; i < e; ++i) {
+            int64_t tot = 0;
+            for (int t = 0; t < nch; ++t) tot += cur[t][i];
+            ptr[i + 1] = tot;
+        }
+    });
+    for (int64_t i = 0; i < rows; ++i) ptr[i + 1] += ptr[i];
+    parallel_chunks(nch, rows, 1 << 14, [&](int64_t b, int64_t e, int) {
+        for (int64_t i = b; i < e; ++i) {
+            int64_t off = ptr[i];
+            for (int t = 0; t < nch; ++t) {
+                const int64_t cnt = cur[t][i];
+                cur[t][i] = off;
+                off += cnt;
+            }
+        }
+    });
+    runs([&](int t) {
+        const int64_t b = std::min(nnz, t * per), e = std::min(nnz, b + per);
+        int64_t* cu = cur[t].data();
+        for (int64_t k = b; k < e; ++k) {
+            const int64_t p = cu[r[k]]++;
+            idx[p] = c[k];
+            val[p] = v[k];
+        }
+    });
 }
 
 // Rows sorted by length, longest first, inside windows of `window` rows; the
 // window keeps neighbouring rows together so gathers keep their locality.
-std::vector<int32_t> sigma_sort(const std::vector<int64_t>& ptr, int window) {
+std::vector<int32_t> sigma_sort(const std::vector<int64_t>& ptr, int window, int threads = 1) {
     const int32_t rows = (int32_t)ptr.size() - 1;
     std::vector<int32_t> perm(rows);
     std::iota(perm.begin(), perm.end(), 0);
     if (window <= 1) return perm;
-    for (int32_t w0 = 0; w0 < rows; w0 += window) {
-        int32_t w1 = std::min<int64_t>((int64_t)w0 + window, rows);
-        std::stable_sort(perm.begin() + w0, perm.begin() + w1, [&](int32_t a, int32_t b) {
-            return ptr[a + 1] - ptr[a] > ptr[b + 1] - ptr[b];
-        });
-    }
+    const int64_t windows = ((int64_t)rows + window - 1) / window;
+    parallel_chunks(threads, windows, 64, [&](int64_t wb, int64_t we, int) {
+        for (int64_t wi = wb; wi < we; ++wi) {
+            const int64_t w0 = wi * window, w1 = std::min<int64_t>(w0 + window, rows);
+            std::stable_sort(perm.begin() + w0, perm.begin() + w1, [&](int32_t a, int32_t b) {
+                return ptr[a + 1] - ptr[a] > ptr[b + 1] - ptr[b];
+            });
+        }
+    });
     return perm;
 }
 
@@ -259,11 +346,17 @@ void build_layout(const b2_lp_view& U, const b2_lp_view& S, const double* Dr, co
     if ((n > 0 && (!U.c || !U.l || !U.u || !S.c || !S.l || !S.u || !Dc)) ||
         (m > 0 && (!U.rL || !U.rU || !S.rL || !Dr)))
         fail(B2_ERR_INVALID, "null vector pointer");
-    for (int64_t k = 0; k < nnz; ++k) {
+    const int th = std::max(1, bp.threads);
+    // the entries are checked in parallel; the first bad one is reported
+    const int64_t bad = first_bad(th, nnz, [&](int64_t k) {
+        return U.row_idx[k] < 0 || U.row_idx[k] >= m || U.col_idx[k] < 0 || U.col_idx[k] >= n ||
+               !std::isfinite(U.val[k]) || !std::isfinite(S.val[k]);
+    });
+    if (bad >= 0) {
+        const int64_t k = bad;
         if (U.row_idx[k] < 0 || U.row_idx[k] >= m || U.col_idx[k] < 0 || U.col_idx[k] >= n)
             fail(B2_ERR_INVALID, "matrix index out of range at entry " + std::to_string(k));
-        if (!std::isfinite(U.val[k]) || !std::isfinite(S.val[k]))
-            fail(B2_ERR_NONFINITE, "non-finite matrix value at entry " + std::to_string(k));
+        fail(B2_ERR_NONFINITE, "non-finite matrix value at entry " + std::to_string(k));
     }
     // PDLP-form invariant (src/pdlp.cpp:59-62): rL finite, rU == rL or +inf.
     for (int32_t i = 0; i < m; ++i) {
@@ -272,41 +365,41 @@ void build_layout(const b2_lp_view& U, const b2_lp_view& S, const double* Dr, co
             fail(B2_ERR_INVALID, "row " + std::to_string(i) + " is neither an equality nor a >= row");
         if (!(Dr[i] > 0) || !std::isfinite(Dr[i])) fail(B2_ERR_INVALID, "Dr must be positive and finite");
     }
-    for (int32_t j = 0; j < n; ++j) {
+    auto col_bad = [&](int64_t j) {
+        const double want = Dc[j] * U.c[j];
+        return !std::isfinite(U.c[j]) || !std::isfinite(S.c[j]) || std::isnan(U.l[j]) || std::isnan(U.u[j]) ||
+               U.l[j] > U.u[j] || !(Dc[j] > 0) || !std::isfinite(Dc[j]) ||
+               std::fabs(S.c[j] - want) > 1e-9 * (1.0 + std::fabs(want));
+    };
+    const int64_t jb = first_bad(th, n, col_bad);
+    if (jb >= 0) {
+        const int64_t j = jb;
         if (!std::isfinite(U.c[j]) || !std::isfinite(S.c[j])) fail(B2_ERR_NONFINITE, "non-finite cost at column " + std::to_string(j));
         if (std::isnan(U.l[j]) || std::isnan(U.u[j]) || U.l[j] > U.u[j])
             fail(B2_ERR_INVALID, "bad bounds at column " + std::to_string(j));
         if (!(Dc[j] > 0) || !std::isfinite(Dc[j])) fail(B2_ERR_INVALID, "Dc must be positive and finite");
-        const double want = Dc[j] * U.c[j];
-        if (std::fabs(S.c[j] - want) > 1e-9 * (1.0 + std::fabs(want)))
-            fail(B2_ERR_INVALID, "scaled cost is not Dc * cost at column " + std::to_string(j));
+        fail(B2_ERR_INVALID, "scaled cost is not Dc * cost at column " + std::to_string(j));
     }
 
     L.m = m; L.n = n; L.nnz = nnz;
     std::vector<int64_t> aptr, tptr;
     std::vector<int32_t> aidx, tidx;
     std::vector<double> aval, tval;
-    {
-        // A and A^T are independent: two threads when the caller allows
-        std::thread ta;
-        if (bp.threads > 1) ta = std::thread([&] { coo_to_csr(m, nnz, U.row_idx, U.col_idx, U.val, aptr, aidx, aval); });
-        else coo_to_csr(m, nnz, U.row_idx, U.col_idx, U.val, aptr, aidx, aval);
-        coo_to_csr(n, nnz, U.col_idx, U.row_idx, U.val, tptr, tidx, tval);
-        if (ta.joinable()) ta.join();
-    }
+    coo_to_csr(m, nnz, U.row_idx, U.col_idx, U.val, aptr, aidx, aval, th);
+    coo_to_csr(n, nnz, U.col_idx, U.row_idx, U.val, tptr, tidx, tval, th);
 
-    L.exact32 = true;
-    for (int64_t k = 0; k < nnz; ++k)
-        if ((double)(float)U.val[k] != U.val[k]) { L.exact32 = false; break; }
+    L.exact32 = first_bad(th, nnz, [&](int64_t k) { return (double)(float)U.val[k] != U.val[k]; }) < 0;
 
     const int window = bp.sigma_window > 0 ? bp.sigma_window : 1024;
     const int target = bp.lane_target > 0 ? bp.lane_target : 16;
-    L.perm_r = sigma_sort(aptr, window);
-    L.perm_c = sigma_sort(tptr, window);
+    L.perm_r = sigma_sort(aptr, window, th);
+    L.perm_c = sigma_sort(tptr, window, th);
     L.inv_r.assign(m, 0);
     L.inv_c.assign(n, 0);
     for (int32_t i = 0; i < m; ++i) L.inv_r[L.perm_r[i]] = i;
-    for (int32_t j = 0; j < n; ++j) L.inv_c[L.perm_c[j]] = j;
+    parallel_chunks(th, n, 1 << 16, [&](int64_t b, int64_t e, int) {
+        for (int64_t j = b; j < e; ++j) L.inv_c[L.perm_c[j]] = (int32_t)j;
+    });
 
     if (bp.threads > 1) {
         BuildParams half = bp;
@@ -328,18 +421,27 @@ void build_layout(const b2_lp_view& U, const b2_lp_view& S, const double* Dr, co
         L.dr2[i] = (U.rL[o] != U.rU[o]) ? -w : w;
     }
     L.c.resize(n); L.l.resize(n); L.u.resize(n); L.dc2.resize(n); L.x0.resize(n);
-    for (int32_t j = 0; j < n; ++j) {
-        const int32_t o = L.perm_c[j];
-        L.c[j] = U.c[o];
-        L.l[j] = U.l[o];
-        L.u[j] = U.u[o];
-        L.dc2[j] = Dc[o] * Dc[o];
-        // initial point of include/pdlp_algo.hpp:69, mapped to unscaled space
-        L.x0[j] = Dc[o] * std::min(std::max(0.0, S.l[o]), S.u[o]);
-    }
-    // step size and primal weight seeds (include/pdlp_algo.hpp:70-77), on the scaled form
+    parallel_chunks(th, n, 1 << 16, [&](int64_t b, int64_t e, int) {
+        for (int64_t j = b; j < e; ++j) {
+            const int32_t o = L.perm_c[j];
+            L.c[j] = U.c[o];
+            L.l[j] = U.l[o];
+            L.u[j] = U.u[o];
+            L.dc2[j] = Dc[o] * Dc[o];
+            // initial point of include/pdlp_algo.hpp:69, mapped to unscaled space
+            L.x0[j] = Dc[o] * std::min(std::max(0.0, S.l[o]), S.u[o]);
+        }
+    });
+    // step size and primal weight seeds (include/pdlp_algo.hpp:70-77), on the
+    // scaled form; a maximum does not depend on the order it is taken in
+    std::vector<double> amax_t((size_t)th, 0.0);
+    parallel_chunks(th, nnz, 1 << 16, [&](int64_t b, int64_t e, int t) {
+        double a = 0.0;
+        for (int64_t k = b; k < e; ++k) a = std::max(a, std::fabs(S.val[k]));
+        amax_t[t] = a;
+    });
     double amax = 0.0;
-    for (int64_t k = 0; k < nnz; ++k) amax = std::max(amax, std::fabs(S.val[k]));
+    for (double a : amax_t) amax = std::max(amax, a);
     L.eta0 = amax > 0 ? 1.0 / amax : 1.0;
     double cn = 0.0, bn = 0.0;
     for (int32_t j = 0; j < n; ++j) cn += S.c[j] * S.c[j];
@@ -352,6 +454,41 @@ void build_layout(const b2_lp_view& U, const b2_lp_view& S, const double* Dr, co
     L.denom_p = 1.0 + std::max(finite_inf_norm(U.rL, m), finite_inf_norm(U.rU, m));
     L.denom_d = 1.0 + finite_inf_norm(U.c, n);
     L.obj_offset = U.obj_offset;
+}
+
+// FNV-1a over every array and scalar of a layout: two layouts with the same
+// digest hand the device the same bytes.
+uint64_t layout_digest(const Layout& L) {
+    uint64_t h = 1469598103934665603ull;
+    auto mix = [&](const void* p, size_t bytes) {
+        const unsigned char* b = static_cast<const unsigned char*>(p);
+        for (size_t i = 0; i < bytes; ++i) h = (h ^ b[i]) * 1099511628211ull;
+    };
+    auto vec = [&](const auto& v) {
+        const uint64_t len = v.size();
+        mix(&len, sizeof(len));
+        if (!v.empty()) mix(v.data(), v.size() * sizeof(v[0]));
+    };
+    auto sell = [&](const SellHost& S) {
+        mix(&S.n_rows, sizeof(S.n_rows));
+        mix(&S.n_cols, sizeof(S.n_cols));
+        vec(S.slice); vec(S.col); vec(S.val32); vec(S.val64); vec(S.seg);
+        mix(&S.padded, sizeof(S.padded));
+        mix(&S.seg_slots, sizeof(S.seg_slots));
+        mix(&S.seg_max, sizeof(S.seg_max));
+    };
+    mix(&L.m, sizeof(L.m));
+    mix(&L.n, sizeof(L.n));
+    mix(&L.nnz, sizeof(L.nnz));
+    vec(L.perm_r); vec(L.perm_c); vec(L.inv_r); vec(L.inv_c);
+    sell(L.A);
+    sell(L.AT);
+    const char e32 = L.exact32 ? 1 : 0;
+    mix(&e32, 1);
+    vec(L.b); vec(L.rU); vec(L.dr2); vec(L.c); vec(L.l); vec(L.u); vec(L.x0); vec(L.dc2);
+    const double sc[5] = {L.eta0, L.omega0, L.denom_p, L.denom_d, L.obj_offset};
+    mix(sc, sizeof(sc));
+    return h;
 }
 
 // ----------------------------------------------------------------- scaling

@@ -79,6 +79,7 @@ struct BuildParams {
 // Validates the PDLP form and builds the device layout. Throws Error.
 void build_layout(const b2_lp_view& U, const b2_lp_view& S, const double* Dr, const double* Dc,
                   const BuildParams& bp, Layout& L);
+uint64_t layout_digest(const Layout& L);
 
 void scale_lp(const b2_lp_view& lp, int ruiz_passes, double* val_s, double* c_s, double* rL_s, double* rU_s,
               double* l_s, double* u_s, double* Dr, double* Dc);

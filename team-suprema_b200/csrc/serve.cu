@@ -475,6 +475,7 @@ struct ServerImpl {
         if (o.lane_target > 0) bp.lane_target = o.lane_target;
         if (o.sigma_window > 0) bp.sigma_window = o.sigma_window;
         bp.split = (int64_t)r.val.size() >= so.grid_nnz;  // the whole-GPU lane lays out as b2_engine does
+        if (bp.split) bp.threads = (int)std::max(1u, std::min(8u, std::thread::hardware_concurrency()));
         Layout L;
         build_layout(U, S, Dr.data(), Dc.data(), bp, L);
         r.meta.m = L.m; r.meta.n = L.n; r.meta.nnz = L.nnz;

@@ -102,3 +102,46 @@ def test_random_lp_is_feasible_by_construction():
     assert r["converged"]
     v = O.verify(as_form(U), r["x"], r["y"])
     assert max(v["eps_P"], v["eps_D"], v["eps_G"]) <= 1e-7
+
+
+def _layout_cases():
+    cases = [load_fixture(n) for n in ("afiro", "israel", "share1b")]
+    # sizes that cut every parallel stage into several chunks (entries, sigma
+    # windows, columns) as well as small ones that stay on one thread
+    for lp in (B.gen_random_lp(30_000, 90_000, 8, 3, True), B.gen_random_lp(150_000, 300_000, 4, 5, True),
+               B.gen_transport(300, 200, 2),
+               B.gen_random_lp(2_000, 5_000, 6, 4, False)):
+        U, S, Dr, Dc, _ = B.prepare(lp)
+        cases.append((U, S, Dr, Dc))
+    return cases
+
+
+@pytest.mark.parametrize("whole_gpu", [True, False])
+def test_layout_does_not_depend_on_host_threads(whole_gpu):
+    """The device layout (CSR builds, sigma sort, tuned and split slices,
+    permuted vectors, step seeds) is built on several host threads for the
+    one-LP engine; every thread count must hand the device the same bytes."""
+    for U, S, Dr, Dc in _layout_cases():
+        d1 = B.layout_digest(U, S, Dr, Dc, threads=1, whole_gpu=whole_gpu)
+        for t in (2, 3, 8):
+            assert B.layout_digest(U, S, Dr, Dc, threads=t, whole_gpu=whole_gpu) == d1, (U.m, U.n, t)
+
+
+def test_layout_errors_name_the_first_bad_entry_at_any_thread_count():
+    U, S, Dr, Dc, _ = B.prepare(B.gen_random_lp(30_000, 90_000, 8, 3, True))
+    for bad in (5, 400_000):
+        V = B.RangedLP.like(U)
+        V.col = V.col.copy()
+        V.col[bad] = U.n + 1
+        V.col[bad + 1000] = -1
+        for t in (1, 8):
+            with pytest.raises(B.B2Error) as e:
+                B.layout_digest(V, S, Dr, Dc, threads=t)
+            assert e.value.code == B.B2_ERR_INVALID
+            assert f"entry {bad}" in str(e.value)
+    V = B.RangedLP.like(U)
+    V.val = V.val.copy()
+    V.val[7] = np.nan
+    with pytest.raises(B.B2Error) as e:
+        B.layout_digest(V, S, Dr, Dc, threads=8)
+    assert e.value.code == B.B2_ERR_NONFINITE and "entry 7" in str(e.value)
