@@ -34,6 +34,7 @@ __device__ void fill_params(KParamsBase& P, const BatchArgs& B, const LpDev& d) 
     P.AT = d.AT;
     P.b = d.b; P.rU = d.rU; P.dr2 = d.dr2;
     P.c = d.c; P.l = d.l; P.u = d.u; P.dc2 = d.dc2; P.x0 = d.x0;
+    P.lu_const = d.lu_const; P.l_all = d.l_all; P.u_all = d.u_all;
     P.itf = d.itf;
     P.xsum = d.xsum; P.ysum = d.ysum;
     P.best_x = d.best_x; P.best_y = d.best_y;
@@ -487,6 +488,7 @@ struct BatchImpl {
             q.ctl = ctl + i;
             q.denom_p = li.denom_p; q.denom_d = li.denom_d;
             q.exact32 = li.exact32 ? 1 : 0;
+            q.lu_const = li.lu_const ? 1 : 0; q.l_all = li.l_all; q.u_all = li.u_all;
         }
         B.lps = up(lps);
         B.abort = alloc<int>(1);

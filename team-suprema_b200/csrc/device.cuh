@@ -116,6 +116,9 @@ struct KParamsBase {
     SellDev A, AT;
     const double *b, *rU, *c, *l, *u, *x0;
     const double *dr2, *dc2;  // Dr^2 (negated on >= rows), Dc^2
+    // every column has the same bounds (l_all, u_all): l and u are not read
+    int lu_const;
+    double l_all, u_all;
     Bufs<float> itf;          // FP32 iterates (read when resuming in FP64)
     double *xsum, *ysum, *best_x, *best_y, *out_x, *out_y;
     const int32_t *perm_r, *perm_c;
@@ -146,7 +149,8 @@ struct LpDev {
     double *xsum, *ysum, *best_x, *best_y, *out_x, *out_y;
     Ctl* ctl;
     double denom_p, denom_d;
-    int exact32, pad;
+    int exact32, lu_const;
+    double l_all, u_all;  // the bounds of every column when lu_const
 };
 
 // The CTAs that cooperate on one LP, and this CTA's place in them.
@@ -553,10 +557,23 @@ __device__ __forceinline__ void primal_col_w(int j, T xv, double g, double tau, 
     dx2 += d * d / w;
 }
 
+// Bounds of column j: two loads, or none when every column has the same.
+__device__ __forceinline__ void col_bounds(const KParamsBase& P, int j, double& lj, double& uj) {
+    if (P.lu_const) {
+        lj = P.l_all;
+        uj = P.u_all;
+    } else {
+        lj = __ldg(P.l + j);
+        uj = __ldg(P.u + j);
+    }
+}
+
 template <class T>
 __device__ __forceinline__ void primal_col(const KParams<T>& P, int j, T xv, double g, double tau, T* xn,
                                            double& dx2, T* xs) {
-    primal_col_w<T>(j, xv, g, tau, xn, dx2, xs, __ldg(P.dc2 + j), __ldg(P.c + j), __ldg(P.l + j), __ldg(P.u + j));
+    double lj, uj;
+    col_bounds(P, j, lj, uj);
+    primal_col_w<T>(j, xv, g, tau, xn, dx2, xs, __ldg(P.dc2 + j), __ldg(P.c + j), lj, uj);
 }
 
 // --------------------------------------------------------------- passes
@@ -629,8 +646,7 @@ __device__ void pass_cols_step(const KParams<T>& P, const Ctl& c, const Group& g
                 xv = ld_it<GK>(x + j);
                 w = __ldg(P.dc2 + j);
                 cj = __ldg(P.c + j);
-                lj = __ldg(P.l + j);
-                uj = __ldg(P.u + j);
+                col_bounds(P, j, lj, uj);
             }
             T acc = slice_dot<GK, T, V, T>(P.AT, vb, sl, lane, y);
             if (!seg_finish<GK, T>(P.AT, sl, lane, acc, g)) continue;
@@ -710,7 +726,9 @@ __device__ void pass_cols_check(const KParams<T>& P, const Ctl& c, const Group& 
             const double xa = has_avg ? ld_it<GK>(P.xsum + j) / wsum : xc;
             const double ga = has_avg ? acc / wsum : gc;
             atya[j] = (T)ga;
-            const double cc = __ldg(P.c + j), l = __ldg(P.l + j), u = __ldg(P.u + j);
+            const double cc = __ldg(P.c + j);
+            double l, u;
+            col_bounds(P, j, l, u);
             kkt_col(l, u, cc, xc, cc - gc, v + 0);
             kkt_col(l, u, cc, xa, cc - ga, v + 5);
             const double w = __ldg(P.dc2 + j), xl = (double)ld_it<GK>(P.it.x_last + j);

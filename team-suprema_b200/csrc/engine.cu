@@ -87,11 +87,22 @@ void cuda_ok(cudaError_t e, const char* what) {
 
 namespace {
 
-template <class T>
-T* upload(const std::vector<T>& h, size_t& total) {
-    T* d = dalloc<T>(h.size(), total);
-    if (!h.empty()) cuda_ok(cudaMemcpy(d, h.data(), h.size() * sizeof(T), cudaMemcpyHostToDevice), "upload");
-    return d;
+// Device memory of one-LP engines comes from the device's stream-ordered pool,
+// which keeps freed blocks (release threshold: all): the drop-in call creates
+// and destroys an engine per solve, and the next one then reuses the blocks
+// with no driver allocation or unmapping. A request the pool cannot meet
+// first hands the cached blocks back to the driver and tries once more.
+void* pool_alloc(size_t bytes, cudaMemPool_t pool, cudaStream_t st) {
+    void* p = nullptr;
+    cudaError_t e = cudaMallocFromPoolAsync(&p, bytes, pool, st);
+    if (e == cudaErrorMemoryAllocation) {
+        cudaGetLastError();
+        cuda_ok(cudaStreamSynchronize(st), "sync");
+        cuda_ok(cudaMemPoolTrimTo(pool, 0), "cudaMemPoolTrimTo");
+        e = cudaMallocFromPoolAsync(&p, bytes, pool, st);
+    }
+    cuda_ok(e, "cudaMallocFromPoolAsync");
+    return p;
 }
 
 }  // namespace
@@ -121,21 +132,30 @@ struct EngineImpl {
     int max_ctas = 0;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
 
+    cudaMemPool_t mpool = nullptr;
+
     template <class T>
     T* alloc(size_t n) {
-        T* p = dalloc<T>(n, bytes);
+        const size_t b = (n > 0 ? n : 1) * sizeof(T);
+        T* p = static_cast<T*>(pool_alloc(b, mpool, stream));
         allocs.push_back(p);
+        bytes += b;
         return p;
     }
     template <class T>
     T* up(const std::vector<T>& h) {
-        T* p = upload(h, bytes);
-        allocs.push_back(p);
+        T* p = alloc<T>(h.size());
+        if (!h.empty())
+            cuda_ok(cudaMemcpyAsync(p, h.data(), h.size() * sizeof(T), cudaMemcpyHostToDevice, stream), "upload");
         return p;
     }
 
     ~EngineImpl() {
-        for (void* p : allocs) cudaFree(p);
+        // back to the pool in stream order (every solve has finished: solves block)
+        if (stream) {
+            for (void* p : allocs) cudaFreeAsync(p, stream);
+            cudaStreamSynchronize(stream);
+        }
         if (h_stop) cudaFreeHost(h_stop);
         if (ev0) cudaEventDestroy(ev0);
         if (ev1) cudaEventDestroy(ev1);
@@ -163,7 +183,7 @@ struct EngineImpl {
             d.seg = reinterpret_cast<const int2*>(up(S.seg));
             d.seg_part = alloc<double>((size_t)S.seg_slots * 32);
             unsigned* cnt = alloc<unsigned>((size_t)S.n_groups());
-            cuda_ok(cudaMemset(cnt, 0, sizeof(unsigned) * (size_t)S.n_groups()), "memset");
+            cuda_ok(cudaMemsetAsync(cnt, 0, sizeof(unsigned) * (size_t)S.n_groups(), stream), "memset");
             d.seg_cnt = cnt;
         }
         return d;
@@ -201,6 +221,9 @@ struct EngineImpl {
         cuda_ok(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking), "cudaStreamCreate");
         cuda_ok(cudaEventCreate(&ev0), "event");
         cuda_ok(cudaEventCreate(&ev1), "event");
+        cuda_ok(cudaDeviceGetDefaultMemPool(&mpool, device), "cudaDeviceGetDefaultMemPool");
+        uint64_t keep = ~uint64_t(0);
+        cuda_ok(cudaMemPoolSetAttribute(mpool, cudaMemPoolAttrReleaseThreshold, &keep), "cudaMemPoolSetAttribute");
         A = upload_sell(L.A);
         AT = upload_sell(L.AT);
         b = up(L.b); rU = up(L.rU); dr2 = up(L.dr2);
@@ -249,6 +272,7 @@ struct EngineImpl {
         P.m = L.m; P.n = L.n;
         P.A = A; P.AT = AT;
         P.b = b; P.rU = rU; P.c = c; P.l = l; P.u = u; P.x0 = x0; P.dr2 = dr2; P.dc2 = dc2;
+        P.lu_const = L.lu_const ? 1 : 0; P.l_all = L.l_all; P.u_all = L.u_all;
         P.it = B;
         P.itf = itf;
         P.xsum = xsum; P.ysum = ysum; P.best_x = best_x; P.best_y = best_y; P.out_x = out_x; P.out_y = out_y;

@@ -432,6 +432,13 @@ void build_layout(const b2_lp_view& U, const b2_lp_view& S, const double* Dr, co
             L.x0[j] = Dc[o] * std::min(std::max(0.0, S.l[o]), S.u[o]);
         }
     });
+    // one pair of bounds for every column (bitwise): the kernels then read no l, u
+    L.lu_const = n > 0 && first_bad(th, n, [&](int64_t j) {
+                              return std::memcmp(&L.l[j], &L.l[0], sizeof(double)) != 0 ||
+                                     std::memcmp(&L.u[j], &L.u[0], sizeof(double)) != 0;
+                          }) < 0;
+    L.l_all = n > 0 ? L.l[0] : 0.0;
+    L.u_all = n > 0 ? L.u[0] : 0.0;
     // step size and primal weight seeds (include/pdlp_algo.hpp:70-77), on the
     // scaled form; a maximum does not depend on the order it is taken in
     std::vector<double> amax_t((size_t)th, 0.0);
@@ -483,8 +490,11 @@ uint64_t layout_digest(const Layout& L) {
     vec(L.perm_r); vec(L.perm_c); vec(L.inv_r); vec(L.inv_c);
     sell(L.A);
     sell(L.AT);
-    const char e32 = L.exact32 ? 1 : 0;
+    const char e32 = L.exact32 ? 1 : 0, luc = L.lu_const ? 1 : 0;
     mix(&e32, 1);
+    mix(&luc, 1);
+    mix(&L.l_all, sizeof(double));
+    mix(&L.u_all, sizeof(double));
     vec(L.b); vec(L.rU); vec(L.dr2); vec(L.c); vec(L.l); vec(L.u); vec(L.x0); vec(L.dc2);
     const double sc[5] = {L.eta0, L.omega0, L.denom_p, L.denom_d, L.obj_offset};
     mix(sc, sizeof(sc));

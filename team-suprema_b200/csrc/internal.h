@@ -59,6 +59,8 @@ struct Layout {
     // cols
     std::vector<double> c, l, u, x0;  // x0 = Dc * clamp(0, l_s, u_s)
     std::vector<double> dc2;          // Dc^2
+    bool lu_const = false;            // every column has the bounds (l_all, u_all), bit for bit
+    double l_all = 0.0, u_all = 0.0;
     // scalars
     double eta0 = 1.0, omega0 = 1.0, denom_p = 1.0, denom_d = 1.0, obj_offset = 0.0;
 };

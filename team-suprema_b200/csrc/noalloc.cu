@@ -195,6 +195,7 @@ void solve_noalloc(const b2_lp_view& U, const b2_lp_view& S, const double* Dr, c
         P.m = L.m; P.n = L.n;
         P.A = A; P.AT = AT;
         P.b = b; P.rU = rU; P.c = cc; P.l = l; P.u = u; P.x0 = x0; P.dr2 = dr2; P.dc2 = dc2;
+        P.lu_const = L.lu_const ? 1 : 0; P.l_all = L.l_all; P.u_all = L.u_all;
         P.it = B;
         P.itf = itf;
         P.xsum = xsum; P.ysum = ysum; P.best_x = best_x; P.best_y = best_y; P.out_x = out_x; P.out_y = out_y;

@@ -133,6 +133,8 @@ struct LpMeta {
     int64_t nnz = 0, a_slices = 0, at_slices = 0;
     bool exact32 = true;
     double denom_p = 1.0, denom_d = 1.0;
+    bool lu_const = false;
+    double l_all = 0.0, u_all = 0.0;
 };
 
 dev::LpDev region_desc(unsigned char* base, const RegionPlan& r, const LpMeta& M) {
@@ -161,6 +163,7 @@ dev::LpDev region_desc(unsigned char* base, const RegionPlan& r, const LpMeta& M
     d.ctl = reinterpret_cast<dev::Ctl*>(base + r.ctl);
     d.denom_p = M.denom_p; d.denom_d = M.denom_d;
     d.exact32 = M.exact32 ? 1 : 0;
+    d.lu_const = M.lu_const ? 1 : 0; d.l_all = M.l_all; d.u_all = M.u_all;
     return d;
 }
 
@@ -482,6 +485,7 @@ struct ServerImpl {
         r.meta.a_slices = L.A.n_slices(); r.meta.at_slices = L.AT.n_slices();
         r.meta.exact32 = L.exact32;
         r.meta.denom_p = L.denom_p; r.meta.denom_d = L.denom_d;
+        r.meta.lu_const = L.lu_const; r.meta.l_all = L.l_all; r.meta.u_all = L.u_all;
         r.grid = bp.split;
         r.cluster = !r.grid && so.cluster_nnz > 0 && L.A.padded + L.AT.padded >= so.cluster_nnz;
         r.plan = plan_region(L);
