@@ -52,7 +52,7 @@ REF_ATTEMPTS = {"large": 143360, "medium": 73024, "small": 13888}
 # 256-attempt solves of the workload (FP32 iterates, FP64 iterates); the roofline's `traffic`
 # scales them by the attempts of each timed launch. Command and figures:
 # profiles/k_pdlp_traffic_random_1M_cols.md.
-TRAFFIC_PER_ATTEMPT = {"large": (150.9e6, 203.9e6)}
+TRAFFIC_PER_ATTEMPT = {"large": (139.6e6, 170.2e6)}
 
 
 def describe(name, count=0, seconds=0.0, world=1):
