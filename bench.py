@@ -238,6 +238,62 @@ def reference_arm(args, world, rank):
 _ref_problem_cache = {}
 
 
+def _form_arrays(U):
+    return (U.m, U.n, U.row, U.col, U.val, U.c, U.rL, U.rU, U.l, U.u, U.obj_offset)
+
+
+def _ref_warm(_i=0):
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    O.reference()
+    time.sleep(0.3)  # held long enough that every worker process takes one
+    return os.getpid()
+
+
+def _ref_solve(arrs):
+    """One full solve by the reference CPU PDLP (solve_pdhg, src/pdlp.cpp:146)
+    in a pool worker: (seconds of the solve by the reference's clock, attempts,
+    converged)."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    m, n, row, col, val, c, rL, rU, l, u, off = arrs
+    P = O.RefProblem.from_form(O.LPForm(m, n, row, col, val, c, rL, rU, l, u, off), use_presolve=False)
+    r = P.solve_pdhg(max_iterations=2_000_000, check_every=64, tol=1e-6)
+    return r["seconds"], r["iterations"], r["converged"]
+
+
+def cpu_all_cores(B, lps, budget_s):
+    """The reference CPU PDLP on every host core: independent single-threaded
+    solves, one spawned process per core, of the LPs in `lps` (unscaled PDLP
+    forms, in order) until budget_s of wall time has passed (solves already
+    started finish). Returns (solves/s, dict): the rate is cores x solved
+    LPs / the sum of their solve seconds, i.e. the cores kept busy all the
+    time, an upper bound on what the CPU sustains on this mix."""
+    import concurrent.futures as cf
+    import multiprocessing as mp
+    cores = os.cpu_count() or 1
+    with cf.ProcessPoolExecutor(max_workers=cores, mp_context=mp.get_context("spawn")) as ex:
+        list(ex.map(_ref_warm, range(cores)))  # every worker up and the library loaded before the clock
+        t0 = time.perf_counter()
+        pending, it = set(), iter(lps)
+        out = []
+        while True:
+            while len(pending) < cores and time.perf_counter() - t0 < budget_s:
+                U = next(it, None)
+                if U is None:
+                    break
+                pending.add(ex.submit(_ref_solve, _form_arrays(U)))
+            if not pending:
+                break
+            fin, pending = cf.wait(pending, return_when=cf.FIRST_COMPLETED)
+            out.extend(f.result() for f in fin)
+        wall = time.perf_counter() - t0
+    solved = [o for o in out if o[2]]
+    busy = sum(o[0] for o in out)
+    rate = cores * len(solved) / busy if busy > 0 else 0.0
+    return rate, {"cores": cores, "lps": len(out), "converged": len(solved), "busy_s": busy, "wall_s": wall}
+
+
 def cpu_sample(O, U, iters):
     key = id(U)
     if key not in _ref_problem_cache:
@@ -307,6 +363,14 @@ def batch_bench(args, world, rank, local):
     lat = sorted(r["device_ms"] for r in res)
     conv = int(dist_sum(sum(r["converged"] for r in res), world))
     attempts = np.array([r["iterations"] for r in res])
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        # the batch's LPs are drawn independently, so its first ones are a sample of the mix
+        rate, st = cpu_all_cores(B, [pr[0] for pr in probs], args.cpu_budget_s)
+        cpu = {"value": rate, "unit": UNIT, "cores": st["cores"], "kind": "reference",
+               "sample": f"the reference solve_pdhg to 1e-6 on the batch's first {st['lps']} LPs, one process per "
+                         f"core ({st['converged']} converged; {st['busy_s']:.1f} s of solves in {st['wall_s']:.1f} s); "
+                         "solves/s = cores x LPs / solve seconds"}
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
@@ -325,7 +389,7 @@ def batch_bench(args, world, rank, local):
             "converged": conv, "attempts": {"median": float(np.median(attempts)), "max": int(attempts.max()),
                                             "total": int(attempts.sum())},
             "clocks": clk.summary(), "gpu_launches": args.steps, "prep_s": t_prep, "create_s": t_create,
-            "device_bytes": info["device_bytes"],
+            "device_bytes": info["device_bytes"], "cpu_baseline": cpu,
         }
         print(json.dumps(line), flush=True)
     bt.close()
@@ -399,6 +463,9 @@ def serve_bench(args, world, rank, local):
     lanes = [info["lane"] for _, info in out]
     sizes = np.array([m for (_, m, *_rest) in stream])
     sizes_all = np.array([m for (_, m, *_rest) in full])
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = serve_cpu_baseline(B, stream, lps, out)
     if rank == 0:
         q = lambda a, f: float(np.quantile(a, f)) if len(a) else None  # noqa: E731
         line = {
@@ -421,10 +488,102 @@ def serve_bench(args, world, rank, local):
             "converged": int(conv), "worst_kkt": worst, "whole_gpu_lane": int(sum(lanes)),
             "server": {"rounds": st1["rounds"] - st0["rounds"], "grid_slices": st1["grid_slices"] - st0["grid_slices"],
                        "busy_ms": st1["busy_ms"] - st0["busy_ms"], "peak_bytes": st1["peak_bytes"]},
-            "wall_s": wall, "gen_s": t_gen, "clocks": clk.summary(),
+            "wall_s": wall, "gen_s": t_gen, "clocks": clk.summary(), "cpu_baseline": cpu,
             "gpu_launches": int(st1["rounds"] - st0["rounds"] + st1["grid_slices"] - st0["grid_slices"]),
         }
         print(json.dumps(line), flush=True)
+
+
+def serve_cpu_baseline(B, stream, lps, out):
+    """The reference CPU PDLP serving the whole stream on every host core,
+    estimated per size class: the larger requests take a CPU minutes
+    (m <= 50,000) to hours (m = 500,000) each, too long to run. Up to three
+    requests per class get two bounded runs (8 and 40 attempts, one core),
+    which give the class's set-up and time per attempt; a request's CPU time
+    is set-up + its attempts (the attempts this engine's served answer took)
+    x time per attempt. With C cores the stream needs at least
+    max(sum / C, longest request) seconds."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    if not O.reference_available():
+        return None
+    cores = os.cpu_count() or 1
+    sizes = np.array([m for (_, m, *_r) in stream])
+    classes = {"m<=2000": sizes <= 2000, "2000<m<500000": (sizes > 2000) & (sizes < 500_000),
+               "m=500000": sizes >= 500_000}
+    times = np.zeros(len(stream))
+    model = {}
+    for name, mask in classes.items():
+        idx = np.flatnonzero(mask)
+        if idx.size == 0:
+            continue
+        setups, pers = [], []
+        for i in idx[np.linspace(0, idx.size - 1, min(3, idx.size)).astype(int)]:
+            U = B.prepare(lps[i])[0]
+            P = O.RefProblem.from_form(O.LPForm(*_form_arrays(U)), use_presolve=False)
+            r1 = P.solve_pdhg(max_iterations=8, check_every=64, tol=1e-6)
+            r2 = P.solve_pdhg(max_iterations=40, check_every=64, tol=1e-6)
+            per = (r2["seconds"] - r1["seconds"]) / max(1, r2["iterations"] - r1["iterations"])
+            setups.append(max(0.0, r1["seconds"] - r1["iterations"] * per))
+            pers.append(per)
+        setup, per = float(np.mean(setups)), float(np.mean(pers))
+        for i in idx:
+            times[i] = setup + out[i][0].iterations * per
+        model[name] = {"requests": int(idx.size), "ms_per_attempt": per * 1e3, "cpu_s": float(times[idx].sum())}
+    span = max(times.sum() / cores, times.max())
+    return {"value": float(len(stream) / span), "unit": UNIT, "cores": cores, "kind": "reference",
+            "sample": f"per size class, bounded runs (8 and 40 attempts) of the reference solve_pdhg on up to 3 "
+                      f"requests; each request = set-up + its attempts x time per attempt; the stream on {cores} "
+                      f"cores takes max(sum / cores, longest) = {span:.1f} s",
+            "classes": model}
+
+
+def reference_many(args, world, rank):
+    """--impl reference for the batch and the served stream: the reference CPU
+    PDLP as independent single-threaded solves on every host core (the
+    reference solves one LP per call and has no batching or serving); each
+    step is a bounded sample of the workload's LPs."""
+    if rank != 0:
+        return None
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import b200pdlp as B
+    import oracle as O
+    if not O.reference_available():
+        return {"impl": "reference", "unavailable": "reference CPU engine not built (oracle/_ref/libsovref.so)"}
+    kind, p = WORKLOADS[args.workload]
+    if kind == "batch":
+        shapes = batch_shapes(B, args.workload, args.batch_count, args.batch_mhi, 1)
+        gen = ((m, n, k, sd) for (m, n, k, sd) in shapes)
+        what = "the batch's LPs in order"
+    else:
+        stream = serve_stream(p["rate"], args.serve_seconds or p["seconds"], p["seed"])
+        gen = ((m, n, k, sd) for (_, m, n, k, sd) in stream if m <= 2000)
+        what = "the stream's m <= 2000 requests in arrival order (an upper bound for the whole mix)"
+    rates, stats = [], []
+    for _ in range(args.warmup + args.steps):
+        lps = []
+        for (m, n, k, sd) in gen:
+            lps.append(B.prepare(B.gen_random_lp(m, n, k, sd, True))[0])
+            if len(lps) >= 4 * (os.cpu_count() or 1):
+                break
+        if not lps:
+            break
+        r, st = cpu_all_cores(B, lps, args.cpu_budget_s)
+        rates.append(r)
+        stats.append(st)
+    timed = rates[args.warmup:] or rates[-1:]
+    value = float(np.mean(timed))
+    cb = {"value": value, "unit": UNIT, "cores": stats[-1]["cores"], "kind": "reference",
+          "sample": f"per step up to {4 * stats[-1]['cores']} of {what}, solve_pdhg to 1e-6, one process per core "
+                    f"for about {args.cpu_budget_s:.0f} s; solves/s = cores x LPs / solve seconds"}
+    cfg = {"workload": describe(args.workload, count=args.batch_count, seconds=args.serve_seconds),
+           "parallelism": f"{stats[-1]['cores']} host cores, one solve per core"}
+    return {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus, "steps": len(timed),
+            "warmup": args.warmup, "ms_per_step": 1e3 / value if value > 0 else None, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic", "impl": "reference",
+            "config": cfg, "cpu_baseline": cb,
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "steps_detail": stats}
 
 
 def profile_mode(args):
@@ -461,6 +620,8 @@ def main():
                     help="attempts per solve used to turn the reference's attempts/s into solves/s "
                          "(0: take the engine's own count from a solve of this LP)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-budget-s", type=float, default=15.0,
+                    help="batch / serve: wall seconds of the all-cores reference CPU sample (per step)")
     ap.add_argument("--mode", default="bench", choices=["bench", "spmv", "solve"],
                     help="spmv / solve: one short run of that kernel for profiling (ncu), no JSON line")
     ap.add_argument("--max-attempts", type=int, default=256, help="--mode solve: attempt limit")
@@ -476,6 +637,11 @@ def main():
     world, rank, local = dist_setup(args.gpus)
     if args.mode != "bench":
         return profile_mode(args)
+    if args.impl == "reference" and WORKLOADS[args.workload][0] in ("batch", "serve"):
+        line = reference_many(args, world, rank)
+        if rank == 0 and line is not None:
+            print(json.dumps(line), flush=True)
+        return
     if WORKLOADS[args.workload][0] == "batch":
         return batch_bench(args, world, rank, local)
     if WORKLOADS[args.workload][0] == "serve":
