@@ -144,7 +144,11 @@ int b2_solve_pdhg_gpu_noalloc(const b2_lp_view* unscaled_form, const b2_lp_view*
 /* ---- resident engine: upload once, solve many times ---------------------
  * b2_engine_create does what the reference's GpuBackend constructor does
  * (gpu/pdlp_gpu_solve.cu:198-205): builds the device layout of A and A^T and
- * uploads the problem. b2_engine_solve then runs from HBM-resident data. */
+ * uploads the problem. b2_engine_solve then runs from HBM-resident data.
+ * Engine memory (and so that of b2_solve_pdhg_gpu, which makes an engine per
+ * call) comes from the device's default stream-ordered memory pool, whose
+ * release threshold is raised so that freed blocks stay cached for the next
+ * engine; cudaMemPoolTrimTo on that pool hands them back to the driver. */
 typedef struct b2_engine b2_engine;
 
 int b2_engine_create(const b2_lp_view* unscaled_form, const b2_lp_view* scaled_form, const double* Dr,
