@@ -7,8 +7,11 @@ reference verifier). One step = one full solve from a cold start.
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
 Prints ONE JSON line (rank 0). Under torchrun with N > 1 every rank solves its
-own replica of the LP (a single LP does not shard) and `value`
-is the total solves/s of the job, timed as the max over ranks.
+own replica of the LP (one LP is not partitioned: that would need an exchange
+of x' and y' every attempt) and `value` is the total solves/s of the job, timed
+as the max over ranks. The batch and the served stream (--workload batch|serve)
+are sharded instead: every rank takes its share from the same deterministic
+plan (b2_shard_plan), with no collective on the data path.
 """
 from __future__ import annotations
 
