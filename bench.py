@@ -736,7 +736,7 @@ def main():
     d2h = 8 * (m + n)
 
     cpu = None
-    if rank == 0 and not args.no_cpu_baseline:
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
             sys.path.insert(0, os.path.join(ROOT, "oracle"))
             import oracle as O
