@@ -1,11 +1,13 @@
 // capi.cpp -- the extern "C" boundary of libb200pdlp.so (include/b200_pdlp.h).
 // Every entry point converts internal errors into a B2_ERR_* status plus a
 // thread-local message; no exception crosses the ABI.
+#include <algorithm>
 #include <chrono>
 #include <cstring>
 #include <exception>
 #include <new>
 #include <string>
+#include <thread>
 
 #include "b200_pdlp.h"
 #include "internal.h"
@@ -382,7 +384,8 @@ int b2_scale(const b2_lp_view* lp, int32_t ruiz_passes, double* val_s, double* c
              double* l_s, double* u_s, double* Dr, double* Dc) {
     return b2::guarded([&] {
         if (!lp) b2::fail(B2_ERR_INVALID, "null argument");
-        b2::scale_lp(*lp, ruiz_passes, val_s, c_s, rL_s, rU_s, l_s, u_s, Dr, Dc);
+        b2::scale_lp(*lp, ruiz_passes, val_s, c_s, rL_s, rU_s, l_s, u_s, Dr, Dc,
+                     (int)std::max(1u, std::min(8u, std::thread::hardware_concurrency())));
     });
 }
 

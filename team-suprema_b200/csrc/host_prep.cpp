@@ -502,16 +502,135 @@ uint64_t layout_digest(const Layout& L) {
 }
 
 // ----------------------------------------------------------------- scaling
-void scale_lp(const b2_lp_view& lp, int ruiz_passes, double* val_s, double* c_s, double* rL_s, double* rU_s,
-              double* l_s, double* u_s, double* Dr, double* Dc) {
+namespace {
+
+// Entry positions k grouped by key (rows or columns), each group in
+// increasing k: the order in which the serial loop adds a group's entries.
+void stable_groups(int64_t groups, int64_t nnz, const int32_t* key, int threads, std::vector<int64_t>& ptr,
+                   std::vector<int64_t>& pos) {
+    // a stable counting sort, as in coo_to_csr: contiguous entry runs counted
+    // per group, turned into per-run offsets (earlier runs first), scattered
+    ptr.assign(groups + 1, 0);
+    pos.resize(nnz);
+    const int nch = (int)std::max<int64_t>(1, std::min<int64_t>(std::max(1, threads), nnz / (1 << 18)));
+    const int64_t per = (nnz + nch - 1) / nch;
+    std::vector<std::vector<int64_t>> cur((size_t)nch);
+    auto runs = [&](auto&& body) {
+        std::vector<std::thread> pool;
+        for (int t = 1; t < nch; ++t) pool.emplace_back([&body, t] { body(t); });
+        body(0);
+        for (auto& th : pool) th.join();
+    };
+    runs([&](int t) {
+        cur[t].assign((size_t)groups, 0);
+        const int64_t b = std::min(nnz, t * per), e = std::min(nnz, b + per);
+        for (int64_t k = b; k < e; ++k) cur[t][key[k]]++;
+    });
+    for (int64_t i = 0; i < groups; ++i) {
+        int64_t off = ptr[i];
+        for (int t = 0; t < nch; ++t) {
+            const int64_t c = cur[t][i];
+            cur[t][i] = off;
+            off += c;
+        }
+        ptr[i + 1] = off;
+    }
+    runs([&](int t) {
+        const int64_t b = std::min(nnz, t * per), e = std::min(nnz, b + per);
+        int64_t* cu = cur[t].data();
+        for (int64_t k = b; k < e; ++k) pos[cu[key[k]]++] = k;
+    });
+}
+
+// The scaling of scale_lp on several threads, with the serial loops' bits:
+// maxima and products do not depend on the order they are taken in, and the
+// Pock-Chambolle sums add every row's (column's) entries in increasing k, as
+// the serial loop does.
+void scale_lp_parallel(const b2_lp_view& lp, int ruiz_passes, int th, double* val_s, double* Dr, double* Dc,
+                       std::vector<double>& rs, std::vector<double>& cs) {
     const int32_t m = lp.m, n = lp.n;
     const int64_t nnz = lp.nnz;
-    for (int64_t k = 0; k < nnz; ++k)
-        if (lp.row_idx[k] < 0 || lp.row_idx[k] >= m || lp.col_idx[k] < 0 || lp.col_idx[k] >= n)
-            fail(B2_ERR_INVALID, "matrix index out of range");
+    const int32_t* R = lp.row_idx;
+    const int32_t* Cc = lp.col_idx;
+    const int64_t grain = 1 << 16;
+    std::vector<std::vector<double>> part((size_t)th);
+    // per-thread maxima over contiguous entry runs, then the maximum of those
+    auto group_max = [&](const int32_t* key, int64_t groups, std::vector<double>& out) {
+        const int nch = parallel_chunks(th, nnz, grain, [&](int64_t b, int64_t e, int t) {
+            std::vector<double>& p = part[t];
+            p.assign((size_t)groups, 0.0);
+            for (int64_t k = b; k < e; ++k) p[key[k]] = std::max(p[key[k]], std::fabs(val_s[k]));
+        });
+        parallel_chunks(th, groups, grain, [&](int64_t b, int64_t e, int) {
+            for (int64_t i = b; i < e; ++i) {
+                double v = 0.0;
+                for (int t = 0; t < nch; ++t) v = std::max(v, part[t][i]);
+                out[i] = v > 0 ? 1.0 / std::sqrt(v) : 1.0;
+            }
+        });
+    };
+    for (int pass = 0; pass < ruiz_passes; ++pass) {
+        group_max(R, m, rs);
+        parallel_chunks(th, nnz, grain, [&](int64_t b, int64_t e, int) {
+            for (int64_t k = b; k < e; ++k) val_s[k] = val_s[k] * rs[R[k]];
+        });
+        for (int32_t i = 0; i < m; ++i) Dr[i] *= rs[i];
+        group_max(Cc, n, cs);
+        parallel_chunks(th, nnz, grain, [&](int64_t b, int64_t e, int) {
+            for (int64_t k = b; k < e; ++k) val_s[k] = val_s[k] * cs[Cc[k]];
+        });
+        for (int32_t j = 0; j < n; ++j) Dc[j] *= cs[j];
+    }
+    std::vector<int64_t> ptr, pos;
+    auto group_sum = [&](const int32_t* key, int64_t groups, std::vector<double>& out) {
+        stable_groups(groups, nnz, key, th, ptr, pos);
+        parallel_chunks(th, groups, grain / 16, [&](int64_t b, int64_t e, int) {
+            for (int64_t i = b; i < e; ++i) {
+                double v = 0.0;
+                for (int64_t p = ptr[i]; p < ptr[i + 1]; ++p) v += std::fabs(val_s[pos[p]]);
+                out[i] = std::sqrt(v > 0 ? 1.0 / v : 1.0);
+            }
+        });
+    };
+    group_sum(R, m, rs);
+    group_sum(Cc, n, cs);
+    parallel_chunks(th, nnz, grain, [&](int64_t b, int64_t e, int) {
+        for (int64_t k = b; k < e; ++k) val_s[k] = val_s[k] * rs[R[k]] * cs[Cc[k]];
+    });
+}
+
+}  // namespace
+
+void scale_lp(const b2_lp_view& lp, int ruiz_passes, double* val_s, double* c_s, double* rL_s, double* rU_s,
+              double* l_s, double* u_s, double* Dr, double* Dc, int threads) {
+    const int32_t m = lp.m, n = lp.n;
+    const int64_t nnz = lp.nnz;
+    const int th = std::max(1, threads);
+    if (first_bad(th, nnz, [&](int64_t k) {
+            return lp.row_idx[k] < 0 || lp.row_idx[k] >= m || lp.col_idx[k] < 0 || lp.col_idx[k] >= n;
+        }) >= 0)
+        fail(B2_ERR_INVALID, "matrix index out of range");
     const int32_t* R = lp.row_idx;
     const int32_t* Cc = lp.col_idx;
     std::copy(lp.val, lp.val + nnz, val_s);
+    if (th > 1 && nnz >= (1 << 18)) {
+        std::fill(Dr, Dr + m, 1.0);
+        std::fill(Dc, Dc + n, 1.0);
+        std::vector<double> rs(m), cs(n);
+        scale_lp_parallel(lp, ruiz_passes, th, val_s, Dr, Dc, rs, cs);
+        for (int32_t i = 0; i < m; ++i) Dr[i] *= rs[i];
+        for (int32_t j = 0; j < n; ++j) Dc[j] *= cs[j];
+        for (int32_t j = 0; j < n; ++j) {
+            c_s[j] = Dc[j] * lp.c[j];
+            l_s[j] = lp.l[j] / Dc[j];
+            u_s[j] = lp.u[j] / Dc[j];
+        }
+        for (int32_t i = 0; i < m; ++i) {
+            rL_s[i] = Dr[i] * lp.rL[i];
+            rU_s[i] = Dr[i] * lp.rU[i];
+        }
+        return;
+    }
     std::fill(Dr, Dr + m, 1.0);
     std::fill(Dc, Dc + n, 1.0);
     std::vector<double> rs(m), cs(n);

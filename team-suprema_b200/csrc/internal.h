@@ -83,8 +83,9 @@ void build_layout(const b2_lp_view& U, const b2_lp_view& S, const double* Dr, co
                   const BuildParams& bp, Layout& L);
 uint64_t layout_digest(const Layout& L);
 
+// Ruiz + Pock-Chambolle on the host; the same bits with any number of threads.
 void scale_lp(const b2_lp_view& lp, int ruiz_passes, double* val_s, double* c_s, double* rL_s, double* rU_s,
-              double* l_s, double* u_s, double* Dr, double* Dc);
+              double* l_s, double* u_s, double* Dr, double* Dc, int threads = 1);
 
 // The same scaling on the GPU, bit for bit (scale.cu).
 void scale_lp_gpu(const b2_lp_view& lp, int ruiz_passes, double* val_s, double* c_s, double* rL_s, double* rU_s,

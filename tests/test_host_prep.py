@@ -31,6 +31,27 @@ def test_product_scaling_random_family():
     np.testing.assert_array_equal(dc, dc2)
 
 
+@pytest.mark.parametrize("shape", [(150_000, 300_000, 4, 21, True), (2_500, 1_000_000, None, 3, None)])
+def test_product_scaling_on_threads_is_bitexact(shape):
+    """From 262,144 entries b2_scale runs on several threads (per-thread
+    maxima, row and column sums in COO order through stable orders); the bits
+    must still be the serial restatement's. One random LP and a transport LP
+    (1M columns of 2 entries, rows of 500 and 2,000)."""
+    m, n, k, seed, fp32 = shape
+    lp = B.gen_random_lp(m, n, k, seed, fp32) if k else B.gen_transport(2000, 500, seed)
+    assert lp.nnz >= 1 << 18
+    s, dr, dc = B.scale(lp)
+    s2, dr2, dc2 = O.scale(as_form(lp))
+    np.testing.assert_array_equal(s.val, s2.val)
+    np.testing.assert_array_equal(s.c, s2.c)
+    np.testing.assert_array_equal(s.l, s2.l)
+    np.testing.assert_array_equal(s.u, s2.u)
+    np.testing.assert_array_equal(s.rL, s2.rL)
+    np.testing.assert_array_equal(s.rU, s2.rU)
+    np.testing.assert_array_equal(dr, dr2)
+    np.testing.assert_array_equal(dc, dc2)
+
+
 def _mixed_rows_lp():
     # rows: E, L, G, ranged, free, E ; columns with finite / infinite bounds
     rng = np.random.default_rng(5)
