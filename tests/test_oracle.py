@@ -82,3 +82,29 @@ def test_restatement_small_random_lp_matches_reference_objective():
     obj = float(np.dot(U.c, r["x"]))
     ref = g["simplex"]["objective"]
     assert abs(obj - ref) / max(1.0, abs(ref)) < 1e-6
+
+
+@pytest.mark.parametrize("kind", ["random", "transport"])
+def test_generated_lp_round_trips_through_the_reference_mps_reader(kind, tmp_path):
+    """Generated benchmark LPs are handed to the reference's own tools as MPS
+    (%.17g, written by oracle/ref_capi.cpp): the reference's read_mps must give
+    back the same LP, value for value."""
+    import b200pdlp as B
+    if not O.reference_available():
+        pytest.skip("oracle/_ref is not built")
+    lp = B.gen_random_lp(300, 900, 6, 5, False) if kind == "random" else B.gen_transport(40, 30, 2)
+    P = O.RefProblem.from_form(O.LPForm(lp.m, lp.n, lp.row, lp.col, lp.val, lp.c, lp.rL, lp.rU, lp.l, lp.u),
+                               use_presolve=False)
+    path = str(tmp_path / "gen.mps")
+    P.write_mps(path)
+    a = P.form(P.ORIGINAL)
+    b = O.RefProblem.from_mps(path, use_presolve=False).form(O.RefProblem.ORIGINAL)
+    assert (a.m, a.n, a.nnz) == (b.m, b.n, b.nnz)
+    ka = np.lexsort((a.col, a.row))
+    kb = np.lexsort((b.col, b.row))
+    np.testing.assert_array_equal(a.row[ka], b.row[kb])
+    np.testing.assert_array_equal(a.col[ka], b.col[kb])
+    np.testing.assert_array_equal(a.val[ka], b.val[kb])
+    for f in ("c", "rL", "rU", "l", "u"):
+        np.testing.assert_array_equal(getattr(a, f), getattr(b, f))
+    assert a.obj_offset == b.obj_offset
