@@ -108,3 +108,22 @@ def test_generated_lp_round_trips_through_the_reference_mps_reader(kind, tmp_pat
     for f in ("c", "rL", "rU", "l", "u"):
         np.testing.assert_array_equal(getattr(a, f), getattr(b, f))
     assert a.obj_offset == b.obj_offset
+
+
+@pytest.mark.skipif(not O.reference_available(), reason="reference library not built here")
+@pytest.mark.parametrize("seed", range(2, 10))
+def test_restatement_bitexact_with_reference_c0_seed_sweep(seed):
+    """The 600 x 1,800 random LP (6 nonzeros per column, FP64 values, the CPU
+    configuration) over a sweep of seeds: the restatement takes the reference's
+    solve_pdhg steps to 1e-6, bit for bit, and converges with it."""
+    import b200pdlp as B
+    lp = B.gen_random_lp(600, 1800, 6, seed, False)
+    U, S, Dr, Dc, _ = B.prepare(lp)
+    fU = O.LPForm(U.m, U.n, U.row, U.col, U.val, U.c, U.rL, U.rU, U.l, U.u, U.obj_offset)
+    fS = O.LPForm(S.m, S.n, S.row, S.col, S.val, S.c, S.rL, S.rU, S.l, S.u, S.obj_offset)
+    r = O.pdlp_run(fU, fS, Dr, Dc, max_iterations=500000, tol=1e-6)
+    ref = O.RefProblem.from_form(fU, use_presolve=False).solve_pdhg(max_iterations=500000, tol=1e-6)
+    assert r["converged"] and ref["converged"]
+    assert ref["iterations"] == r["iterations"] and ref["restarts"] == r["restarts"]
+    np.testing.assert_array_equal(ref["x"], r["x"])
+    np.testing.assert_array_equal(ref["y"], r["y"])
