@@ -111,3 +111,54 @@ def test_noalloc_rejects_lp_above_its_static_limit():
                                             None, None, C.byref(r))
     assert rc == B.B2_ERR_UNSUPPORTED
     assert "32 MiB" in B.lib().b2_last_error().decode()
+
+
+C_CLIENT = r"""
+#include <stdio.h>
+#include <string.h>
+#include "b200_pdlp.h"
+
+int main(void) {
+    /* a plain C caller: version, options, the shard plan and a host-only layout digest */
+    b2_solve_opts o;
+    b2_default_opts(&o);
+    if (o.check_every != 64) return 10;
+    int64_t work[5] = {5, 9, 1, 9, 3};
+    int32_t rank_of[5];
+    if (b2_shard_plan(work, 5, 2, 0, rank_of) != B2_OK) return 11;
+    /* longest first: 9 -> 0, 9 -> 1, 5 -> 0, 3 -> 1, 1 -> 1 */
+    const int32_t want[5] = {0, 0, 1, 1, 1};
+    if (memcmp(rank_of, want, sizeof(want)) != 0) return 12;
+    if (b2_request_work(3, 4, 10) != 27) return 13;
+    /* min x0 + x1 s.t. x0 + x1 = 1, 0 <= x <= 1 (PDLP form, no scaling) */
+    int32_t row[2] = {0, 0}, col[2] = {0, 1};
+    double val[2] = {1.0, 1.0}, c[2] = {1.0, 1.0}, rl[1] = {1.0}, ru[1] = {1.0}, l[2] = {0.0, 0.0},
+           u[2] = {1.0, 1.0}, dr[1] = {1.0}, dc[2] = {1.0, 1.0};
+    b2_lp_view U = {1, 2, 2, row, col, val, c, rl, ru, l, u, 0.0};
+    uint64_t d1 = 0, d2 = 0;
+    if (b2_layout_digest(&U, &U, dr, dc, 1, 1, &d1) != B2_OK) return 14;
+    if (b2_layout_digest(&U, &U, dr, dc, 4, 1, &d2) != B2_OK || d1 != d2) return 15;
+    col[1] = 7; /* out of range: rejected on the host, with a message */
+    if (b2_layout_digest(&U, &U, dr, dc, 1, 1, &d1) != B2_ERR_INVALID) return 16;
+    if (strstr(b2_last_error(), "entry 1") == NULL) return 17;
+    printf("c client ok: %s\n", b2_version());
+    return 0;
+}
+"""
+
+
+def test_header_compiles_as_c_and_a_c_client_runs(tmp_path):
+    """include/b200_pdlp.h is a C header (C99, no C++), and the library is
+    usable from C: host-only calls run here without a GPU."""
+    import subprocess
+    src = tmp_path / "client.c"
+    src.write_text(C_CLIENT)
+    exe = tmp_path / "client"
+    libdir = os.path.dirname(B.LIB_PATH)
+    cmd = ["gcc", "-std=c99", "-Wall", "-Werror", "-pedantic", "-I", os.path.join(ROOT, "include"), str(src),
+           "-o", str(exe), "-L", libdir, "-lb200pdlp", f"-Wl,-rpath,{libdir}"]
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    r = subprocess.run([str(exe)], capture_output=True, text=True, timeout=120)
+    assert r.returncode == 0, (r.returncode, r.stdout, r.stderr)
+    assert "c client ok" in r.stdout
