@@ -243,11 +243,11 @@ def reference_arm(args, world, rank):
     import multiprocessing as mp
     lp = make_lp(B, args.workload)
     U, S, Dr, Dc, _ = B.prepare(lp)
-    # one process per core, as many as host memory holds (a worker keeps its
-    # own copy of the LP and the reference's CSR/CSC of it: ~40 bytes per
-    # nonzero with headroom)
+    # one process per core, as many as half the host memory holds: a worker
+    # keeps its own copy of the LP and the reference's forms of it (1.8 GB
+    # peak for the 8M-nonzero LP; 250 bytes per nonzero leaves headroom)
     mem = os.sysconf("SC_PAGE_SIZE") * os.sysconf("SC_PHYS_PAGES")
-    per_worker = max(1 << 28, 200 * U.nnz)
+    per_worker = max(1 << 28, 250 * U.nnz)
     cores = max(1, min(os.cpu_count() or 1, int(0.5 * mem // per_worker)))
     attempts = args.ref_attempts_per_solve
     per_step, sample_s = [], 0.0
