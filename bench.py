@@ -430,6 +430,9 @@ def batch_bench(args, world, rank, local):
                        else "single GPU"},
             "latency_ms": {"p50": lat[len(lat) // 2], "p99": lat[int(0.99 * (len(lat) - 1))], "max": lat[-1],
                            "note": "per-LP time on its CTA inside the launch (rank 0's share)"},
+            "occupancy": {"lp_ms_sum": float(sum(lat)), "ctas": info["max_ctas"],
+                          "busy_fraction": float(sum(lat)) / (steps[-1][1] * max(1, info["max_ctas"])),
+                          "note": "sum of the LPs' times on their CTAs over (launch time x CTAs), last step"},
             "converged": conv, "attempts": {"median": float(np.median(attempts)), "max": int(attempts.max()),
                                             "total": int(attempts.sum())},
             "clocks": clk.summary(), "gpu_launches": args.steps, "prep_s": t_prep, "create_s": t_create,
