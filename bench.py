@@ -45,16 +45,11 @@ WORKLOADS = {
 }
 
 
-# Attempts the reference algorithm (include/pdlp_algo.hpp) needs to reach 1e-6 on each workload,
-# used to turn the reference CPU engine's measured attempts/s into solves/s. "small" is the
-# reference's own count (tests/golden/golden.json); the others are this engine's FP64-mode
-# count, which takes the reference's decisions (tests/test_gpu_solve.py).
-REF_ATTEMPTS = {"large": 143360, "medium": 73024, "small": 13888}
-
-# DRAM bytes (read + write) per attempt of the persistent solve kernel, from ncu captures of
-# 256-attempt solves of the workload (FP32 iterates, FP64 iterates); the roofline's `traffic`
-# scales them by the attempts of each timed launch. Command and figures:
-# profiles/k_pdlp_traffic_random_1M_cols.md.
+# DRAM bytes (read + write) per attempt of the persistent solve kernel, from one ncu capture
+# (dram__bytes_read.sum + dram__bytes_write.sum) of 256-attempt solves of the workload with FP32
+# and with FP64 iterates (`bench.py --mode solve --max-attempts 256`). A profiler cannot run
+# inside the timed region, so the roofline's `traffic` is this capture scaled by the attempts
+# of each timed launch, and the line labels it so.
 TRAFFIC_PER_ATTEMPT = {"large": (139.6e6, 170.2e6)}
 
 
@@ -209,48 +204,88 @@ def dist_barrier(world: int):
 _ref_worker_problem = None
 
 
+def ref_lp(name):
+    """The workload's LP built by the oracle's restated generators (the same
+    bits as the product's; pinned by tests/test_oracle.py), so the reference
+    arm never loads the product library."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    kind, p = WORKLOADS[name]
+    if kind == "random":
+        return O.gen_random_lp(p["m"], p["n"], p["k"], p["seed"], p["fp32"])
+    return O.gen_transport(p["S"], p["D"], p["seed"])
+
+
+def ref_attempts_per_solve(name):
+    """(attempts, source) one solve of the workload's LP takes at 1e-6 by the
+    reference algorithm, from runs of the reference itself recorded in
+    tests/golden/ (make_golden*.py): its FP64 GPU engine's full solve of the
+    large LP, its CPU engine's full solves of the transportation and small
+    LPs. (None, None) when no reference record exists."""
+    try:
+        big = json.load(open(os.path.join(ROOT, "tests", "golden", "large.json")))
+        small = json.load(open(os.path.join(ROOT, "tests", "golden", "golden.json")))["random"]
+    except (OSError, ValueError, KeyError):
+        return None, None
+    if name == "large" and "gpu_fp64_1e-06" in big.get("large", {}):
+        return int(big["large"]["gpu_fp64_1e-06"]["attempts"]), "reference FP64 GPU engine, full solve"
+    if name == "transport" and "cpu_pdlp_1e-06" in big.get("transport", {}):
+        return int(big["transport"]["cpu_pdlp_1e-06"]["attempts"]), "reference CPU PDLP, full solve"
+    if name == "small" and "rand_m600_n1800_k6_s0_f64" in small:
+        return int(small["rand_m600_n1800_k6_s0_f64"]["pdlp"]["1e-06"]["iterations"]), "reference CPU PDLP, full solve"
+    return None, None
+
+
 def _ref_worker_init(workload):
-    """Pool-worker set-up: the workload's LP (regenerated from its seed: the
-    same bits in every process) handed to the reference as its PDLP form."""
+    """Pool-worker set-up: the workload's raw LP (regenerated from its seed:
+    the same bits in every process) through the reference's own
+    build_pdlp_form -> scale (src/pdlp.cpp:8-82, src/scaling.cpp:25-84), without
+    presolve, i.e. the PDLP form the B200 engine receives."""
     global _ref_worker_problem
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
-    import b200pdlp as B
     import oracle as O
-    U = B.prepare(make_lp(B, workload))[0]
-    _ref_worker_problem = O.RefProblem.from_form(O.LPForm(*_form_arrays(U)), use_presolve=False)
+    _ref_worker_problem = O.RefProblem.from_form(ref_lp(workload), use_presolve=False)
 
 
 def _ref_worker_attempts(iters):
     r = _ref_worker_problem.solve_pdhg(max_iterations=iters, check_every=64, tol=1e-6)
-    return r["seconds"], r["iterations"]
+    return r["seconds"], r["iterations"], r["converged"]
 
 
 def reference_arm(args, world, rank):
     """The reference's own CPU PDLP (solve_pdhg, src/pdlp.cpp:146, built from
     its sources into oracle/_ref) on every host core: the engine is
     single-threaded, so each core runs its own solve of the LP, all at once
-    (they share the memory bandwidth). Each step is a bounded sample of
-    cpu_sample_iters attempts per core; solves/s = the cores' summed
-    attempts/s / the attempts one solve needs."""
+    (they share the memory bandwidth).
+
+    Where one solve fits a step (the small LP), every step is full solves on
+    every core and solves/s is measured. Otherwise each step is a bounded
+    sample of cpu_sample_iters attempts per core; solves/s is then
+    extrapolated from the cores' summed attempts/s with the attempts per solve
+    the reference itself took (ref_attempts_per_solve), and the line says so
+    (extrapolated, sampled_attempts, attempts_per_solve_source). ms_per_step is
+    always the measured wall time of a step."""
     if rank != 0:
         return None
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
-    import b200pdlp as B
     import oracle as O
     if not O.reference_available():
         return {"impl": "reference", "unavailable": "reference CPU engine not built (oracle/_ref/libsovref.so)"}
     import concurrent.futures as cf
     import multiprocessing as mp
-    lp = make_lp(B, args.workload)
-    U, S, Dr, Dc, _ = B.prepare(lp)
+    lp = ref_lp(args.workload)
+    attempts, source = ref_attempts_per_solve(args.workload)
+    full = args.workload == "small"
+    if attempts is None and not full:
+        return {"impl": "reference", "unavailable": f"no reference attempt count recorded for {args.workload}"}
     # one process per core, as many as half the host memory holds: a worker
-    # keeps its own copy of the LP and the reference's forms of it (1.8 GB
-    # peak for the 8M-nonzero LP; 250 bytes per nonzero leaves headroom)
+    # keeps the reference's forms of the LP (1.8 GB peak for the 8M-nonzero
+    # LP; 250 bytes per nonzero leaves headroom)
     mem = os.sysconf("SC_PAGE_SIZE") * os.sysconf("SC_PHYS_PAGES")
-    per_worker = max(1 << 28, 250 * U.nnz)
+    per_worker = max(1 << 28, 250 * lp.nnz)
     cores = max(1, min(os.cpu_count() or 1, int(0.5 * mem // per_worker)))
-    attempts = args.ref_attempts_per_solve
-    per_step, sample_s = [], 0.0
+    iters = 2_000_000 if full else args.cpu_sample_iters
+    per_step, step_ms, solved = [], [], 0
     with cf.ProcessPoolExecutor(max_workers=cores, mp_context=mp.get_context("spawn"),
                                 initializer=_ref_worker_init, initargs=(args.workload,)) as ex:
         # every worker holds its problem before the first step (each answers with its pid)
@@ -259,24 +294,41 @@ def reference_arm(args, world, rank):
             seen |= set(ex.map(_ref_warm, range(cores)))
             if len(seen) >= cores:
                 break
-        for _ in range(args.warmup + args.steps):
-            res = [f.result() for f in [ex.submit(_ref_worker_attempts, args.cpu_sample_iters) for _ in range(cores)]]
-            per_step.append(sum(it / sec for sec, it in res if sec > 0))
-            sample_s = max(sec for sec, _ in res)
+        for s in range(args.warmup + args.steps):
+            t0 = time.perf_counter()
+            res = [f.result() for f in [ex.submit(_ref_worker_attempts, iters) for _ in range(cores)]]
+            wall = time.perf_counter() - t0
+            if full:
+                per_step.append(sum(1 for _, _, ok in res if ok) / wall)
+                if s >= args.warmup:
+                    solved += sum(1 for _, _, ok in res if ok)
+            else:
+                per_step.append(sum(it / sec for sec, it, _ in res if sec > 0))
+            step_ms.append(wall * 1e3)
     timed = per_step[args.warmup:] or per_step[-1:]
-    value = float(np.mean(timed)) / attempts
-    cb = {"value": value, "unit": UNIT, "cores": cores, "kind": "reference",
-          "sample": f"{args.cpu_sample_iters} attempts of solve_pdhg per core per step, {cores} single-threaded "
-                    f"solves of this LP at once; solves/s = summed attempts/s / {attempts} attempts per solve at 1e-6"}
-    cfg = workload_config(args, U, lp)
+    timed_ms = step_ms[args.warmup:] or step_ms[-1:]
+    if full:
+        value = float(np.mean(timed))
+        sample = (f"full solves of solve_pdhg to 1e-6, one per core on {cores} cores per step, "
+                  f"{solved} solved in the timed steps; solves/s measured")
+    else:
+        value = float(np.mean(timed)) / attempts
+        sample = (f"{iters} attempts of solve_pdhg per core per step, {cores} single-threaded solves of this LP at "
+                  f"once; solves/s = summed attempts/s / {attempts} attempts per solve ({source})")
+    cb = {"value": value, "unit": UNIT, "cores": cores, "kind": "reference", "sample": sample}
+    cfg = workload_config(args, lp, None)
     cfg["parallelism"] = f"{cores} host cores, one solve per core"
-    return {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": 1e3 / value,
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": float(np.mean(timed_ms)),
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic", "impl": "reference", "config": cfg,
             "cpu_baseline": cb, "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0,
-                                        "d2h_bytes_per_step": 0}, "sample_seconds": sample_s,
-            "attempts_per_s_per_core": float(np.mean(timed)) / cores}
+                                        "d2h_bytes_per_step": 0},
+            "extrapolated": not full}
+    if not full:
+        line.update(sampled_attempts=iters, attempts_per_solve=attempts, attempts_per_solve_source=source,
+                    attempts_per_s_per_core=float(np.mean(timed)) / cores)
+    return line
 
 
 _ref_problem_cache = {}
@@ -306,7 +358,7 @@ def _ref_solve(arrs):
     return r["seconds"], r["iterations"], r["converged"]
 
 
-def cpu_all_cores(B, lps, budget_s):
+def cpu_all_cores(lps, budget_s):
     """The reference CPU PDLP on every host core: independent single-threaded
     solves, one spawned process per core, of the LPs in `lps` (unscaled PDLP
     forms, in order) until budget_s of wall time has passed (solves already
@@ -356,16 +408,29 @@ def workload_config(args, U, lp):
             "parallelism": f"replicas x{args.gpus}" if args.gpus > 1 else "single GPU"}
 
 
-def batch_shapes(B, name, count=0, m_hi=0, world=1):
+def family_shapes(count: int, seed: int, m_lo: int = 50, m_hi: int = 5000):
+    """The uneven batch family: m log-uniform on [m_lo, m_hi], n = round(U[2,4] m),
+    nonzeros per column uniform on {4..10}, one derived seed per LP; a list of
+    (m, n, k, seed). The same draw as the library's batch_family_shapes (a test
+    pins the two), restated here so the reference arm does not load the library."""
+    rng = np.random.default_rng(seed)
+    m = np.exp(rng.uniform(np.log(m_lo), np.log(m_hi), count)).round().astype(int)
+    n = np.round(rng.uniform(2.0, 4.0, count) * m).astype(int)
+    k = rng.integers(4, 11, count)
+    seeds = rng.integers(0, 2**62, count)
+    return [(int(a), int(b), int(c), int(d)) for a, b, c, d in zip(m, n, k, seeds)]
+
+
+def batch_shapes(name, count=0, m_hi=0, world=1):
     """The batch of `count` LPs per GPU: world x count shapes drawn from one
     master seed (the single-GPU batch is the first draw of the same family)."""
     _, p = WORKLOADS[name]
-    return B.batch_family_shapes((count or p["count"]) * world, p["seed"], m_hi=m_hi or 5000)
+    return family_shapes((count or p["count"]) * world, p["seed"], m_hi=m_hi or 5000)
 
 
 def make_batch(B, name, count=0, m_hi=0, world=1, rank=0):
     """This rank's share of the batch (all of it on one GPU), balanced by load."""
-    shapes = batch_shapes(B, name, count, m_hi, world)
+    shapes = batch_shapes(name, count, m_hi, world)
     mine = my_share(B, [B.request_work(m, n, n * k) for (m, n, k, _) in shapes], world, rank)
     probs = []
     for i in mine:
@@ -410,7 +475,7 @@ def batch_bench(args, world, rank, local):
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         # the batch's LPs are drawn independently, so its first ones are a sample of the mix
-        rate, st = cpu_all_cores(B, [pr[0] for pr in probs], args.cpu_budget_s)
+        rate, st = cpu_all_cores([pr[0] for pr in probs], args.cpu_budget_s)
         cpu = {"value": rate, "unit": UNIT, "cores": st["cores"], "kind": "reference",
                "sample": f"the reference solve_pdhg to 1e-6 on the batch's first {st['lps']} LPs, one process per "
                          f"core ({st['converged']} converged; {st['busy_s']:.1f} s of solves in {st['wall_s']:.1f} s); "
@@ -593,13 +658,12 @@ def reference_many(args, world, rank):
     if rank != 0:
         return None
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
-    import b200pdlp as B
     import oracle as O
     if not O.reference_available():
         return {"impl": "reference", "unavailable": "reference CPU engine not built (oracle/_ref/libsovref.so)"}
     kind, p = WORKLOADS[args.workload]
     if kind == "batch":
-        shapes = batch_shapes(B, args.workload, args.batch_count, args.batch_mhi, 1)
+        shapes = batch_shapes(args.workload, args.batch_count, args.batch_mhi, 1)
         gen = ((m, n, k, sd) for (m, n, k, sd) in shapes)
         what = "the batch's LPs in order"
     else:
@@ -610,15 +674,16 @@ def reference_many(args, world, rank):
     for _ in range(args.warmup + args.steps):
         lps = []
         for (m, n, k, sd) in gen:
-            lps.append(B.prepare(B.gen_random_lp(m, n, k, sd, True))[0])
+            lps.append(O.gen_random_lp(m, n, k, sd, True))
             if len(lps) >= 4 * (os.cpu_count() or 1):
                 break
         if not lps:
             break
-        r, st = cpu_all_cores(B, lps, args.cpu_budget_s)
+        r, st = cpu_all_cores(lps, args.cpu_budget_s)
         rates.append(r)
         stats.append(st)
     timed = rates[args.warmup:] or rates[-1:]
+    timed_wall = [st["wall_s"] for st in (stats[args.warmup:] or stats[-1:])]
     value = float(np.mean(timed))
     cb = {"value": value, "unit": UNIT, "cores": stats[-1]["cores"], "kind": "reference",
           "sample": f"per step up to {4 * stats[-1]['cores']} of {what}, solve_pdhg to 1e-6, one process per core "
@@ -626,7 +691,7 @@ def reference_many(args, world, rank):
     cfg = {"workload": describe(args.workload, count=args.batch_count, seconds=args.serve_seconds),
            "parallelism": f"{stats[-1]['cores']} host cores, one solve per core"}
     return {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus, "steps": len(timed),
-            "warmup": args.warmup, "ms_per_step": 1e3 / value if value > 0 else None, "higher_is_better": True,
+            "warmup": args.warmup, "ms_per_step": 1e3 * float(np.mean(timed_wall)), "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic", "impl": "reference",
             "config": cfg, "cpu_baseline": cb,
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -663,9 +728,6 @@ def main():
     ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])
     ap.add_argument("--e2e-steps", type=int, default=2)
     ap.add_argument("--cpu-sample-iters", type=int, default=40)
-    ap.add_argument("--ref-attempts-per-solve", type=int, default=0,
-                    help="attempts per solve used to turn the reference's attempts/s into solves/s "
-                         "(0: take the engine's own count from a solve of this LP)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-budget-s", type=float, default=15.0,
                     help="batch / serve: wall seconds of the all-cores reference CPU sample (per step)")
@@ -695,8 +757,6 @@ def main():
         return serve_bench(args, world, rank, local)
 
     if args.impl == "reference":
-        if args.ref_attempts_per_solve <= 0:
-            args.ref_attempts_per_solve = REF_ATTEMPTS.get(args.workload, 10_000)
         line = reference_arm(args, world, rank)
         if rank == 0 and line is not None:
             print(json.dumps(line), flush=True)
@@ -786,11 +846,13 @@ def main():
             import oracle as O
             if O.reference_available():
                 s = cpu_sample(O, U, args.cpu_sample_iters)
-                attempts = statistics.median(r.iterations for r in results)
+                attempts, source = ref_attempts_per_solve(args.workload)
+                if attempts is None:
+                    attempts, source = int(statistics.median(r.iterations for r in results)), "this engine's count"
                 cpu = {"value": 1.0 / (s["seconds"] / s["iterations"] * attempts), "unit": UNIT, "cores": 1,
-                       "kind": "reference",
+                       "kind": "reference", "extrapolated": True,
                        "sample": f"{s['iterations']} attempts of the reference solve_pdhg ({s['seconds']:.2f} s) "
-                                 f"on this LP, extrapolated to {attempts} attempts per solve"}
+                                 f"on this LP, extrapolated to {attempts} attempts per solve ({source})"}
         except Exception as e:  # the baseline is reported, not required
             cpu = {"error": str(e)}
 
@@ -811,7 +873,8 @@ def main():
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak_gbs, "unit": "GB/s",
                          "frac": achieved / peak_gbs, "traffic": traffic,
                          "algorithmic_bytes_per_launch": tot_bytes / launches,
-                         "traffic_note": "bytes per launch: ncu DRAM bytes per attempt x the launch's attempts"
+                         "traffic_note": "bytes per launch: DRAM bytes per attempt from an ncu capture of 256-attempt "
+                                         "solves, x the launch's attempts"
                                          if traffic else None,
                          "kernel": "k_pdlp (persistent solve)", "peak_source": peak_src},
             "spmv": {"A_gbs": spmv_gbs, "AT_gbs": spmv_t_gbs, "A_ms": spmv_ms, "AT_ms": spmv_t_ms,

@@ -85,8 +85,31 @@ def restatement():
         lib.or_pdlp_run.argtypes = [C.POINTER(_OrLP), C.POINTER(_OrLP), _f64p, _f64p, C.c_int, C.c_int, C.c_double,
                                     _f64p, _f64p, _i32p, _f64p, C.c_void_p, C.c_int]
         lib.or_pdlp_run.restype = C.c_int
+        lib.or_gen_random_lp.argtypes = [C.c_int, C.c_int, C.c_int, C.c_uint64, C.c_int, _i32p, _i32p] + [_f64p] * 6
+        lib.or_gen_transport.argtypes = [C.c_int, C.c_int, C.c_uint64, _i32p, _i32p] + [_f64p] * 6
         _rest = lib
     return _rest
+
+
+def gen_random_lp(m: int, n: int, k: int, seed: int, fp32_values: bool = True) -> LPForm:
+    """The benchmark's random equality LP (restated generator; the same bits as
+    the product's gen_random_lp, pinned by a content digest in the tests)."""
+    z = n * k
+    row = np.zeros(z, np.int32); col = np.zeros(z, np.int32); val = np.zeros(z)
+    c = np.zeros(n); rL = np.zeros(m); rU = np.zeros(m); l = np.zeros(n); u = np.zeros(n)
+    if restatement().or_gen_random_lp(m, n, k, seed, int(fp32_values), row, col, val, c, rL, rU, l, u):
+        raise ValueError("bad generator sizes")
+    return LPForm(m, n, row, col, val, c, rL, rU, l, u, 0.0)
+
+
+def gen_transport(S: int, D: int, seed: int) -> LPForm:
+    """The benchmark's transportation LP, S sources x D sinks (restated generator)."""
+    n = S * D
+    row = np.zeros(2 * n, np.int32); col = np.zeros(2 * n, np.int32); val = np.zeros(2 * n)
+    c = np.zeros(n); rL = np.zeros(S + D); rU = np.zeros(S + D); l = np.zeros(n); u = np.zeros(n)
+    if restatement().or_gen_transport(S, D, seed, row, col, val, c, rL, rU, l, u):
+        raise ValueError("bad transport sizes")
+    return LPForm(S + D, n, row, col, val, c, rL, rU, l, u, 0.0)
 
 
 def csr(lp: LPForm, transpose: bool = False):

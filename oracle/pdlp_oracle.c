@@ -12,6 +12,8 @@
  *   or_verify      src/verify.cpp:6-103          (verify, finite_inf_norm, vec_norm2)
  *   or_scale       src/scaling.cpp:4-84          (scale, LP case)
  *   or_pdlp_run    include/pdlp_algo.hpp:49-185 with the CPU backend of src/pdlp.cpp:97-142
+ * plus the benchmark LP generators (or_gen_random_lp, or_gen_transport), which
+ * restate this project's own generators, not the reference's.
  */
 #include "pdlp_oracle.h"
 
@@ -368,5 +370,153 @@ int or_pdlp_run(const or_lp* U, const or_lp* S, const double* Dr, const double* 
     free(hxs); free(hys); free(xu); free(yu); free(xu2); free(yu2); free(x_last); free(y_last);
     free(best_x); free(best_y); free(is_ineq);
     free_csr(&Au); free_csr(&AuT); free_csr(&A); free_csr(&AT);
+    return 0;
+}
+
+/* ------------------------------------------------------------ generators
+ * The benchmark LPs are defined by this project's own seeded generators (the
+ * reference's tools/gen_lp.cpp draws different supplies, so they are not the
+ * reference's). These are independent C restatements of the product's
+ * generators (team-suprema_b200/csrc/host_prep.cpp, gen_random_lp and
+ * gen_transport), so that the reference arm of the benchmark and the golden
+ * records can build the same LPs without loading the product library. A test
+ * pins the two to the same content digest. The random source is xoshiro256**
+ * seeded through splitmix64 (Blackman and Vigna's published generators). */
+typedef struct { uint64_t s[4]; } or_rng;
+
+static uint64_t or_rotl(uint64_t x, int k) { return (x << k) | (x >> (64 - k)); }
+
+static void or_rng_seed(or_rng* g, uint64_t seed) {
+    uint64_t z = seed;
+    for (int i = 0; i < 4; ++i) {
+        z += 0x9E3779B97F4A7C15ull;
+        uint64_t t = z;
+        t = (t ^ (t >> 30)) * 0xBF58476D1CE4E5B9ull;
+        t = (t ^ (t >> 27)) * 0x94D049BB133111EBull;
+        g->s[i] = t ^ (t >> 31);
+    }
+}
+
+static uint64_t or_rng_next(or_rng* g) {
+    uint64_t* s = g->s;
+    const uint64_t r = or_rotl(s[1] * 5, 7) * 9;
+    const uint64_t t = s[1] << 17;
+    s[2] ^= s[0];
+    s[3] ^= s[1];
+    s[1] ^= s[2];
+    s[0] ^= s[3];
+    s[2] ^= t;
+    s[3] = or_rotl(s[3], 45);
+    return r;
+}
+
+static double or_uniform(or_rng* g) { return (double)(or_rng_next(g) >> 11) * 0x1.0p-53; }
+static int64_t or_below(or_rng* g, int64_t n) { return (int64_t)(or_uniform(g) * (double)n); }
+
+static double or_normal(or_rng* g) {
+    /* Marsaglia's polar method */
+    for (;;) {
+        double a = 2.0 * or_uniform(g) - 1.0, b = 2.0 * or_uniform(g) - 1.0, q = a * a + b * b;
+        if (q > 0.0 && q < 1.0) return a * sqrt(-2.0 * log(q) / q);
+    }
+}
+
+int or_gen_random_lp(int m, int n, int k, uint64_t seed, int fp32_values, int32_t* row, int32_t* col, double* val,
+                     double* c, double* rL, double* rU, double* l, double* u) {
+    if (m <= 0 || n <= 0 || k <= 0 || k > m) return 1;
+    or_rng g;
+    or_rng_seed(&g, seed);
+    int32_t* pick = (int32_t*)malloc(sizeof(int32_t) * (size_t)k);
+    double* x0 = (double*)malloc(sizeof(double) * (size_t)n);
+    double* y0 = (double*)malloc(sizeof(double) * (size_t)m);
+    for (int32_t j = 0; j < n; ++j) {
+        for (int t = 0; t < k; ++t) {
+            int32_t r;
+            int dup;
+            do { /* k distinct rows per column, uniform */
+                r = (int32_t)or_below(&g, m);
+                dup = 0;
+                for (int q = 0; q < t; ++q) dup |= pick[q] == r;
+            } while (dup);
+            pick[t] = r;
+            double v;
+            do { /* U[-1,1] without zero, optionally rounded to FP32 */
+                v = 2.0 * or_uniform(&g) - 1.0;
+                if (fp32_values) v = (double)(float)v;
+            } while (v == 0.0);
+            const int64_t p = (int64_t)j * k + t;
+            row[p] = r;
+            col[p] = j;
+            val[p] = v;
+        }
+    }
+    for (int32_t j = 0; j < n; ++j) x0[j] = 5.0 * or_uniform(&g);
+    for (int32_t i = 0; i < m; ++i) y0[i] = or_normal(&g);
+    for (int32_t i = 0; i < m; ++i) rL[i] = 0.0;
+    for (int64_t p = 0; p < (int64_t)n * k; ++p) rL[row[p]] += val[p] * x0[col[p]]; /* b = A x0 */
+    for (int32_t j = 0; j < n; ++j) {
+        double s = 0.0;
+        for (int t = 0; t < k; ++t) {
+            const int64_t p = (int64_t)j * k + t;
+            s += val[p] * y0[row[p]];
+        }
+        c[j] = s + or_uniform(&g); /* c = A^T y0 + z0 */
+        l[j] = 0.0;
+        u[j] = 10.0;
+    }
+    for (int32_t i = 0; i < m; ++i) rU[i] = rL[i];
+    free(pick);
+    free(x0);
+    free(y0);
+    return 0;
+}
+
+int or_gen_transport(int S, int D, uint64_t seed, int32_t* row, int32_t* col, double* val, double* c, double* rL,
+                     double* rU, double* l, double* u) {
+    if (S < 1 || D < 1) return 1;
+    or_rng g;
+    or_rng_seed(&g, seed);
+    int64_t* supply = (int64_t*)malloc(sizeof(int64_t) * (size_t)S);
+    int64_t* demand = (int64_t*)malloc(sizeof(int64_t) * (size_t)D);
+    double* w = (double*)malloc(sizeof(double) * (size_t)D);
+    int64_t total = 0, assigned = 0;
+    double wsum = 0.0;
+    for (int i = 0; i < S; ++i) {
+        supply[i] = 100 + or_below(&g, 901);
+        total += supply[i];
+    }
+    for (int j = 0; j < D; ++j) {
+        w[j] = 0.5 + or_uniform(&g);
+        wsum += w[j];
+    }
+    for (int j = 0; j < D; ++j) {
+        int64_t d = (int64_t)floor((double)total * w[j] / wsum);
+        demand[j] = d > 1 ? d : 1;
+        assigned += demand[j];
+    }
+    /* the remainder goes out one unit at a time, round robin, so demands are
+     * an integer partition of the total supply */
+    for (int64_t r = total - assigned, j = 0; r != 0; j = (j + 1) % D) {
+        if (r > 0) { demand[j]++; r--; }
+        else if (demand[j] > 1) { demand[j]--; r++; }
+    }
+    for (int i = 0; i < S; ++i)
+        for (int j = 0; j < D; ++j) {
+            const int64_t a = (int64_t)i * D + j;
+            row[2 * a] = i;
+            col[2 * a] = (int32_t)a;
+            val[2 * a] = 1.0;
+            row[2 * a + 1] = S + j;
+            col[2 * a + 1] = (int32_t)a;
+            val[2 * a + 1] = 1.0;
+            c[a] = (double)(1 + or_below(&g, 100));
+            l[a] = 0.0;
+            u[a] = OR_INF;
+        }
+    for (int i = 0; i < S; ++i) rL[i] = rU[i] = (double)supply[i];
+    for (int j = 0; j < D; ++j) rL[S + j] = rU[S + j] = (double)demand[j];
+    free(supply);
+    free(demand);
+    free(w);
     return 0;
 }

@@ -60,6 +60,18 @@ int or_pdlp_run(const or_lp* unscaled, const or_lp* scaled, const double* Dr, co
                 int max_iterations, int check_every, double tol, double* x, double* y, int* info, double* eps,
                 double* trace, int trace_len);
 
+/* The benchmark LP generators, restated from the product's seeded generators
+ * so that reference-side runs build the same LPs without the product library.
+ * Random equality LP: k distinct rows per column, values U[-1,1] (optionally
+ * rounded to FP32), b = A x0, c = A^T y0 + z0, 0 <= x <= 10; COO of n*k entries
+ * in column order. Transportation LP: S sources x D sinks, 2 unit entries per
+ * arc, integer supplies and demands, integer costs, 0 <= x. Return 0, or 1 on
+ * bad sizes. */
+int or_gen_random_lp(int m, int n, int k, uint64_t seed, int fp32_values, int32_t* row, int32_t* col, double* val,
+                     double* c, double* rL, double* rU, double* l, double* u);
+int or_gen_transport(int S, int D, uint64_t seed, int32_t* row, int32_t* col, double* val, double* c, double* rL,
+                     double* rU, double* l, double* u);
+
 #ifdef __cplusplus
 }
 #endif

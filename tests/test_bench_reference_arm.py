@@ -47,3 +47,35 @@ def test_reference_arm_all_cores(workload):
     check_line(d)
     assert d["cpu_baseline"]["cores"] == (os.cpu_count() or 1)
     assert all(st["converged"] == st["lps"] for st in d["steps_detail"])
+
+
+def test_reference_arm_never_loads_the_product_library():
+    """The reference arm builds its LPs with the oracle's generators and hands
+    them to the reference's own build_pdlp_form -> scale: the product library
+    must not be mapped into its process."""
+    code = ("import runpy, sys; sys.argv = ['bench.py', '--impl', 'reference', '--workload', 'small', '--steps', '1', "
+            "'--warmup', '0']; runpy.run_path('bench.py', run_name='__main__'); "
+            "maps = open('/proc/self/maps').read(); "
+            "print('PRODUCT_MAPPED' if 'libb200pdlp' in maps else 'PRODUCT_NOT_MAPPED'); "
+            "print('ORACLE_MAPPED' if 'liboracle' in maps else 'ORACLE_NOT_MAPPED')")
+    env = dict(os.environ, CUDA_VISIBLE_DEVICES="")
+    out = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True, timeout=600, env=env, cwd=ROOT)
+    assert out.returncode == 0, out.stderr[-2000:]
+    # the LP came from the oracle's generator; the solves ran in spawned workers that import only the oracle
+    assert "PRODUCT_NOT_MAPPED" in out.stdout and "ORACLE_MAPPED" in out.stdout, out.stdout[-2000:]
+
+
+def test_reference_arm_sampled_line_is_labelled_as_extrapolated():
+    d = run_arm("--workload", "transport", "--steps", "1", "--warmup", "0", "--cpu-sample-iters", "4")
+    check_line(d)
+    assert d["extrapolated"] is True and d["sampled_attempts"] == 4
+    assert d["attempts_per_solve_source"].startswith("reference")
+    assert d["ms_per_step"] > 0
+
+
+def test_bench_batch_family_equals_the_library_draw():
+    sys.path.insert(0, ROOT)
+    import bench
+    import b200pdlp as B
+    assert bench.family_shapes(300, 0) == B.batch_family_shapes(300, seed=0)
+    assert bench.family_shapes(50, 5, m_hi=900) == B.batch_family_shapes(50, seed=5, m_hi=900)

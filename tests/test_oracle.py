@@ -4,6 +4,7 @@ built (oracle/_ref) -- against the reference directly, bit for bit."""
 import numpy as np
 import pytest
 
+import b200pdlp
 import oracle as O
 from conftest import fixture_names, golden_index, load_fixture, random_case
 
@@ -70,6 +71,40 @@ def test_random_family_regenerates_bitexact(key):
     from conftest import digest
     lp, *_ , g = random_case(key)
     assert digest(lp) == g["digest"]
+
+
+@pytest.mark.parametrize("key", sorted(golden_index()["random"].keys()))
+def test_oracle_generator_equals_product_generator(key):
+    """The oracle's restated generator (used where the product library must not
+    be loaded: the benchmark's reference arm, the golden records) builds the
+    same LP, bit for bit, as the product's."""
+    from conftest import digest
+    g = golden_index()["random"][key]
+    lp = O.gen_random_lp(g["m"], g["n"], g["k"], g["seed"], g["fp32"])
+    assert digest(lp) == g["digest"]
+    assert digest(lp) == digest(b200pdlp.gen_random_lp(g["m"], g["n"], g["k"], g["seed"], g["fp32"]))
+
+
+@pytest.mark.parametrize("S,D,seed", [(7, 5, 0), (60, 40, 3), (2000, 500, 1)])
+def test_oracle_transport_generator_equals_product_generator(S, D, seed):
+    from conftest import digest
+    assert digest(O.gen_transport(S, D, seed)) == digest(b200pdlp.gen_transport(S, D, seed))
+
+
+def test_large_records_pin_the_generated_lps():
+    """tests/golden/large.json stores the content digests of the benchmark-size
+    LPs the reference solved; the oracle's generator still builds them."""
+    import json
+    import os
+    from conftest import GOLDEN, digest
+    path = os.path.join(GOLDEN, "large.json")
+    if not os.path.exists(path):
+        pytest.skip("no large-LP records")
+    rec = json.load(open(path))
+    p = rec["transport"]["lp"]
+    assert digest(O.gen_transport(p["S"], p["D"], p["seed"])) == rec["transport"]["digest"]
+    p = rec["large"]["lp"]
+    assert digest(O.gen_random_lp(p["m"], p["n"], p["k"], p["seed"], p["fp32"])) == rec["large"]["digest"]
 
 
 def test_restatement_small_random_lp_matches_reference_objective():
