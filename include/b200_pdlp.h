@@ -36,6 +36,8 @@ extern "C" {
 #define B2_ERR_NONFINITE 6   /* NaN / inf where a finite number is required              */
 #define B2_ERR_UNSUPPORTED 7 /* request outside what this build supports                 */
 #define B2_ERR_PENDING 8     /* b2_server_wait: the request has not finished yet          */
+#define B2_ERR_INFEASIBLE 9  /* presolve proved the LP infeasible                          */
+#define B2_ERR_UNBOUNDED 10  /* presolve proved the LP unbounded                           */
 
 /* ---- one LP, as the reference's RangedLP holds it ---------------------
  * rL <= A x <= rU, l <= x <= u, minimise c'x + obj_offset; A in COO
@@ -77,6 +79,13 @@ typedef struct b2_solve_opts {
     int32_t batch_cluster_nnz;/* batches: LPs with at least this many stored entries (A and A^T)
                                  are solved by a cluster of 16 CTAs; <= 0: never (default)     */
     int32_t batch_block;      /* batches: threads per CTA, 128, 256 or 512; 0: auto (512)     */
+    /* Cancellation by callback, for callers whose stop flag is not a plain
+       int32 word (the shim passes a reader of the reference's std::atomic<bool>):
+       while a one-LP solve or a batch runs, the calling thread's wait loop calls
+       stop_poll(stop_ctx) about every 20 us; a nonzero return stops the solve as
+       a set stop_flag does. NULL: not used. */
+    int32_t (*stop_poll)(void* stop_ctx);
+    void* stop_ctx;
 } b2_solve_opts;
 
 void b2_default_opts(b2_solve_opts* opts);
@@ -119,24 +128,29 @@ int b2_solve_pdhg_gpu_ex(const b2_lp_view* unscaled_form, const b2_lp_view* scal
                          double* x_out, double* y_out, b2_result* res);
 
 /* Allocation-free form of b2_solve_pdhg_gpu_ex (no counterpart in the
- * reference). For callers that must not allocate device memory: code running
- * while a CUDA stream is captured into a graph (cudaMalloc is not a capturable
- * stream operation), processes whose GPU memory belongs to a pool they do not
- * own, and latency-critical paths that must stay out of the driver's
- * allocator. It runs the one-CTA solve with its whole device working set
- * (layout, iterates, averages, control state, outputs) in a static device
- * array of 32 MiB that every GPU using the library holds until exit; LPs
- * that need more (roughly above 200,000 nonzeros) get B2_ERR_UNSUPPORTED
- * before any GPU work. It calls no cudaMalloc / cudaFree or other allocating
- * CUDA routine (host memory is still used to build the layout). The first
- * call on a device looks up the array's address with that device current:
- * make that first call before any stream capture starts. All calls in the
- * process share the array, which keeps the previous call's contents (each
- * call clears what must start at zero); calls are serialized by a lock and
- * return after their GPU work ends, since GPU work of two overlapping calls
- * would race on the array. Inputs, outputs and options mean what they mean
- * for b2_solve_pdhg_gpu_ex, except that stop_flag, time limit and stream are
- * not supported (work runs on the legacy default stream). */
+ * reference). For callers that must not allocate device memory: a process
+ * whose GPU memory is reserved up front by another runtime's allocator or a
+ * pool it does not own (so a cudaMalloc from this library would fail or
+ * fragment that pool), and latency-critical paths that must stay out of the
+ * driver's allocator. It runs the one-CTA solve with its whole device working
+ * set (layout, iterates, averages, control state, outputs) in one static
+ * device array of 32 MiB; LPs that need more (roughly above 200,000
+ * nonzeros) get B2_ERR_UNSUPPORTED before any GPU work. It calls no
+ * cudaMalloc / cudaFree or other allocating CUDA routine (host memory is
+ * still used to build the layout). The array's memory: with CUDA's lazy
+ * module loading (the default since CUDA 12.2) a device gets it at the first
+ * call on that device, when the call looks up the array's address
+ * (cudaGetSymbolAddress) with that device current, and keeps it until the
+ * process exits; with eager loading (CUDA_MODULE_LOADING=EAGER) every device
+ * gets it when the library is loaded, whether or not this entry point is
+ * used. Make the first call on a device before any stream capture begins.
+ * The work is issued on the legacy default stream with synchronous copies
+ * and the call returns after its GPU work ends. All calls in the process
+ * share the array, which keeps the previous call's contents (each call
+ * clears what must start at zero); calls are serialized by a process-wide
+ * lock, since GPU work of two calls that overlapped would race on the array.
+ * Inputs, outputs and options mean what they mean for b2_solve_pdhg_gpu_ex,
+ * except that stop_flag, time limit and stream are not supported. */
 int b2_solve_pdhg_gpu_noalloc(const b2_lp_view* unscaled_form, const b2_lp_view* scaled_form, const double* Dr,
                               const double* Dc, const b2_solve_opts* opts, double* x_out, double* y_out,
                               b2_result* res);
@@ -254,6 +268,8 @@ typedef struct b2_request_info {
     int32_t rounds;                   /* rounds (or whole-GPU slices) the LP ran in          */
     int32_t lane;                     /* 0: batched, 1: whole GPU                            */
     int64_t device_bytes;             /* its footprint as admitted                           */
+    double form_eps[3];               /* b2_server_submit_lp: eps_P/D/G of the PDLP form (device) */
+    int32_t presolved_m, presolved_n; /* b2_server_submit_lp: the PDLP form's size           */
 } b2_request_info;
 
 typedef struct b2_server_stats {
@@ -275,6 +291,18 @@ int b2_server_submit(b2_server* s, const b2_lp_view* unscaled_form, int64_t* tic
  * is read and checked on the server's preparation threads, not the caller's.
  * A file that cannot be read or is malformed fails its ticket. */
 int b2_server_submit_file(b2_server* s, const char* path, int64_t* ticket);
+/* Submits an LP as the caller has it (a ranged LP, any row and column
+ * bounds), as src/solve.cpp:150-195 prepares one for PDLP: on the server's
+ * preparation threads it is presolved (when presolve != 0; b2_presolve),
+ * put in PDLP form (b2_pdlp_form_build) and scaled. The answer b2_server_wait
+ * hands over is the original LP's point (x: n, y: m of this LP), mapped back
+ * by extract and postsolve; res->objective is c'x + obj_offset of the
+ * original LP and res->eps_P/D/G are verify()'s figures on the original LP,
+ * computed on the host after postsolve (the PDLP form's device figures are in
+ * b2_request_info.form_eps). An LP that presolve proves infeasible or
+ * unbounded fails its ticket with B2_ERR_INFEASIBLE / B2_ERR_UNBOUNDED; one
+ * that presolve solves outright needs no GPU work. */
+int b2_server_submit_lp(b2_server* s, const b2_lp_view* original, int32_t presolve, int64_t* ticket);
 /* Waits up to timeout_s seconds (< 0: no limit) for a ticket. On B2_OK the
  * result is handed over (x: n, y: m in unscaled PDLP-form space, any may be
  * NULL) and the ticket is forgotten; B2_ERR_PENDING: not finished yet. A
@@ -345,6 +373,33 @@ int b2_scale(const b2_lp_view* lp, int32_t ruiz_passes, double* val_s, double* c
  * does. For ingest of large LPs, whose host scaling takes seconds. */
 int b2_scale_gpu(const b2_lp_view* lp, int32_t ruiz_passes, double* val_s, double* c_s, double* rL_s,
                  double* rU_s, double* l_s, double* u_s, double* Dr, double* Dc);
+
+/* PDLP form of a ranged LP, as build_pdlp_form (src/pdlp.cpp:8-82) builds it:
+ * equality rows first in input order, then the one-sided rows in input order
+ * as A x >= b ("<=" rows negated), a ranged row as an equality with a bounded
+ * slack column (entry -1) after the original columns, free rows dropped. The
+ * form's arrays belong to the b2_pdlp_form; b2_pdlp_form_view points into
+ * them. b2_pdlp_form_extract maps a point of the form (x2: form n, y2: form m)
+ * back to the input LP (x: n, y: m), as extract_solution (src/pdlp.cpp:84-90). */
+typedef struct b2_pdlp_form b2_pdlp_form;
+int b2_pdlp_form_build(const b2_lp_view* ranged, b2_pdlp_form** out);
+void b2_pdlp_form_view(const b2_pdlp_form* f, b2_lp_view* form);
+int b2_pdlp_form_extract(const b2_pdlp_form* f, const double* x2, const double* y2, double* x, double* y);
+void b2_pdlp_form_destroy(b2_pdlp_form* f);
+
+/* Presolve of a ranged LP before the PDLP stage (the role of the reference's
+ * presolve / postsolve, src/presolve.cpp:524-628; this engine's own, smaller
+ * set of reductions: free and empty rows dropped, fixed and empty columns
+ * fixed, singleton rows turned into bounds, repeated to a fixed point).
+ * status: 0 reduced, 1 infeasible, 2 unbounded (then the reduced LP is empty).
+ * b2_presolved_view points into the handle. b2_postsolve maps a point of the
+ * reduced LP (x_red: reduced n, y_red: reduced m) to the original LP (x: n,
+ * y: m), dual values included, so that verify() on the original LP judges it. */
+typedef struct b2_presolved b2_presolved;
+int b2_presolve(const b2_lp_view* original, b2_presolved** out, int32_t* status);
+void b2_presolved_view(const b2_presolved* p, b2_lp_view* reduced);
+int b2_postsolve(const b2_presolved* p, const double* x_red, const double* y_red, double* x, double* y);
+void b2_presolved_destroy(b2_presolved* p);
 
 /* Binary LP request format (no counterpart in the reference, which reads MPS
  * text, src/mps_reader.cpp:66-308): the LP of a b2_lp_view with A in CSR

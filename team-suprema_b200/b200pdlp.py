@@ -32,7 +32,7 @@ LIB_PATH = os.path.join(HERE, "libb200pdlp.so")
 INCLUDE_H = os.path.join(os.path.dirname(HERE), "include", "b200_pdlp.h")
 
 B2_OK, B2_ERR_INVALID, B2_ERR_CUDA, B2_ERR_OOM, B2_ERR_TIMEOUT, B2_ERR_NO_DEVICE, B2_ERR_NONFINITE, \
-    B2_ERR_UNSUPPORTED, B2_ERR_PENDING = range(9)
+    B2_ERR_UNSUPPORTED, B2_ERR_PENDING, B2_ERR_INFEASIBLE, B2_ERR_UNBOUNDED = range(11)
 PREC_FP64, PREC_MIXED = 0, 1
 EXIT_CONVERGED, EXIT_MAX_ITER, EXIT_STOPPED, EXIT_TIME_LIMIT = 1, 2, 3, 4
 
@@ -42,7 +42,9 @@ EXPORTED = [
     "b2_engine_destroy", "b2_engine_get_info", "b2_engine_spmv", "b2_engine_spmv_bench", "b2_engine_trace",
     "b2_batch_create", "b2_batch_solve", "b2_batch_get_solution", "b2_batch_get_info", "b2_batch_spmv",
     "b2_batch_destroy",
-    "b2_server_create", "b2_server_submit", "b2_server_submit_file", "b2_server_wait", "b2_server_stats_get",
+    "b2_server_create", "b2_server_submit", "b2_server_submit_file", "b2_server_submit_lp", "b2_server_wait",
+    "b2_server_stats_get", "b2_pdlp_form_build", "b2_pdlp_form_view", "b2_pdlp_form_extract",
+    "b2_pdlp_form_destroy", "b2_presolve", "b2_presolved_view", "b2_postsolve", "b2_presolved_destroy",
     "b2_server_destroy", "b2_lp_write", "b2_lp_read_dims", "b2_lp_read",
     "b2_layout_digest", "b2_request_work", "b2_shard_plan", "b2_pool_create", "b2_pool_submit", "b2_pool_submit_file",
     "b2_pool_wait", "b2_pool_stats_get", "b2_pool_destroy",
@@ -72,7 +74,7 @@ class SolveOpts(C.Structure):
                 ("time_limit_s", C.c_double), ("barrier_timeout_s", C.c_double), ("max_ctas", C.c_int32),
                 ("lane_target", C.c_int32), ("sigma_window", C.c_int32), ("return_current", C.c_int32),
                 ("stream", C.c_void_p), ("debug_delay_us", C.c_int32), ("batch_cluster_nnz", C.c_int32),
-                ("batch_block", C.c_int32)]
+                ("batch_block", C.c_int32), ("stop_poll", C.c_void_p), ("stop_ctx", C.c_void_p)]
 
 
 class _Result(C.Structure):
@@ -97,7 +99,8 @@ class ServerOpts(C.Structure):
 
 class RequestInfo(C.Structure):
     _fields_ = [("submit_s", C.c_double), ("admit_s", C.c_double), ("done_s", C.c_double),
-                ("prep_ms", C.c_double), ("rounds", C.c_int32), ("lane", C.c_int32), ("device_bytes", C.c_int64)]
+                ("prep_ms", C.c_double), ("rounds", C.c_int32), ("lane", C.c_int32), ("device_bytes", C.c_int64),
+                ("form_eps", C.c_double * 3), ("presolved_m", C.c_int32), ("presolved_n", C.c_int32)]
 
 
 class ServerStats(C.Structure):
@@ -156,6 +159,19 @@ def lib():
             L.b2_server_create.argtypes = [C.POINTER(ServerOpts), C.POINTER(SolveOpts), C.POINTER(vp)]
             L.b2_server_submit.argtypes = [vp, C.POINTER(_LPView), C.POINTER(i64)]
             L.b2_server_submit_file.argtypes = [vp, C.c_char_p, C.POINTER(i64)]
+            L.b2_server_submit_lp.argtypes = [vp, C.POINTER(_LPView), i32, C.POINTER(i64)]
+            L.b2_pdlp_form_build.argtypes = [C.POINTER(_LPView), C.POINTER(vp)]
+            L.b2_pdlp_form_view.argtypes = [vp, C.POINTER(_LPView)]
+            L.b2_pdlp_form_view.restype = None
+            L.b2_pdlp_form_extract.argtypes = [vp, vp, vp, vp, vp]
+            L.b2_pdlp_form_destroy.argtypes = [vp]
+            L.b2_pdlp_form_destroy.restype = None
+            L.b2_presolve.argtypes = [C.POINTER(_LPView), C.POINTER(vp), C.POINTER(i32)]
+            L.b2_presolved_view.argtypes = [vp, C.POINTER(_LPView)]
+            L.b2_presolved_view.restype = None
+            L.b2_postsolve.argtypes = [vp, vp, vp, vp, vp]
+            L.b2_presolved_destroy.argtypes = [vp]
+            L.b2_presolved_destroy.restype = None
             L.b2_lp_write.argtypes = [C.c_char_p, C.POINTER(_LPView)]
             L.b2_lp_read_dims.argtypes = [C.c_char_p, C.POINTER(i32), C.POINTER(i32), C.POINTER(i64)]
             L.b2_lp_read.argtypes = [C.c_char_p] + [vp] * 8 + [C.POINTER(f64)]
@@ -518,6 +534,16 @@ class Server:
         self._dims[t.value] = (U.m, U.n)
         return t.value
 
+    def submit_lp(self, lp: RangedLP, presolve: bool = True) -> int:
+        """Submits an LP as the caller has it (b2_server_submit_lp): presolved,
+        put in PDLP form and scaled on the server's threads; wait() returns the
+        original LP's point (postsolved) with verify()'s figures on it."""
+        L = RangedLP.like(lp)
+        t = C.c_int64()
+        _check(lib().b2_server_submit_lp(self._h, C.byref(L.view()), int(bool(presolve)), C.byref(t)))
+        self._dims[t.value] = (L.m, L.n)
+        return t.value
+
     def submit_file(self, path: str) -> int:
         """Submits an LP stored with write_lp; the server reads it on its own threads."""
         m, n, _ = lp_file_dims(path)
@@ -539,6 +565,7 @@ class Server:
         del self._dims[ticket]
         _check(rc)
         info = {k: getattr(inf, k) for k, _ in RequestInfo._fields_}
+        info["form_eps"] = list(inf.form_eps)
         return _result(r, x[:n], y[:m]), info
 
     def stats(self) -> dict:
@@ -761,6 +788,71 @@ def prepare(lp: RangedLP):
     form, meta = build_pdlp_form(lp)
     scaled, Dr, Dc = scale(form)
     return form, scaled, Dr, Dc, meta
+
+
+def _lp_from_view(v: "_LPView") -> RangedLP:
+    """A copy of the arrays a library-owned view points at."""
+    def arr(p, n, t):
+        return np.ctypeslib.as_array(C.cast(p, C.POINTER(t)), shape=(n,)).copy() if n else np.zeros(0, dtype=t)
+    z = int(v.nnz)
+    return RangedLP(int(v.m), int(v.n), arr(v.row_idx, z, C.c_int32), arr(v.col_idx, z, C.c_int32),
+                    arr(v.val, z, C.c_double), arr(v.c, v.n, C.c_double), arr(v.rL, v.m, C.c_double),
+                    arr(v.rU, v.m, C.c_double), arr(v.l, v.n, C.c_double), arr(v.u, v.n, C.c_double),
+                    float(v.obj_offset))
+
+
+class PdlpForm:
+    """The PDLP form of a ranged LP built by the library (b2_pdlp_form_build,
+    as the reference's build_pdlp_form, src/pdlp.cpp:8-82): .form is the form
+    as a RangedLP; extract(x2, y2) maps a point of the form back to the input LP."""
+
+    def __init__(self, lp: RangedLP):
+        L = RangedLP.like(lp)
+        h = C.c_void_p()
+        _check(lib().b2_pdlp_form_build(C.byref(L.view()), C.byref(h)))
+        self._h, self.m_in, self.n_in = h, L.m, L.n
+        v = _LPView()
+        lib().b2_pdlp_form_view(self._h, C.byref(v))
+        self.form = _lp_from_view(v)
+
+    def extract(self, x2, y2):
+        x = np.zeros(max(self.n_in, 1)); y = np.zeros(max(self.m_in, 1))
+        _check(lib().b2_pdlp_form_extract(self._h, _ptr(_vec(x2, self.form.n)), _ptr(_vec(y2, self.form.m)),
+                                          _ptr(x), _ptr(y)))
+        return x[:self.n_in], y[:self.m_in]
+
+    def __del__(self):
+        if getattr(self, "_h", None) and self._h.value:
+            lib().b2_pdlp_form_destroy(self._h)
+            self._h = C.c_void_p()
+
+
+class Presolved:
+    """b2_presolve: .status (0 reduced, 1 infeasible, 2 unbounded), .reduced
+    (a RangedLP); postsolve(x_red, y_red) maps a point of the reduced LP back
+    to the original LP, dual values included."""
+
+    def __init__(self, lp: RangedLP):
+        L = RangedLP.like(lp)
+        h = C.c_void_p()
+        st = C.c_int32()
+        _check(lib().b2_presolve(C.byref(L.view()), C.byref(h), C.byref(st)))
+        self._h, self.status, self.m0, self.n0 = h, int(st.value), L.m, L.n
+        v = _LPView()
+        lib().b2_presolved_view(self._h, C.byref(v))
+        self.reduced = _lp_from_view(v)
+
+    def postsolve(self, x_red, y_red):
+        x = np.zeros(max(self.n0, 1)); y = np.zeros(max(self.m0, 1))
+        xr = _vec(x_red, self.reduced.n) if self.reduced.n else np.zeros(1)
+        yr = _vec(y_red, self.reduced.m) if self.reduced.m else np.zeros(1)
+        _check(lib().b2_postsolve(self._h, _ptr(xr), _ptr(yr), _ptr(x), _ptr(y)))
+        return x[:self.n0], y[:self.m0]
+
+    def __del__(self):
+        if getattr(self, "_h", None) and self._h.value:
+            lib().b2_presolved_destroy(self._h)
+            self._h = C.c_void_p()
 
 
 def version() -> str:

@@ -553,7 +553,7 @@ struct BatchImpl {
         B.stall_checks = o.stall_checks > 0 ? o.stall_checks : 32;
         B.mixed = o.precision == B2_PREC_MIXED;
         B.round_ns = 0;
-        *h_stop = stop_flag ? *stop_flag : 0;
+        *h_stop = stop_requested(o, stop_flag) ? 1 : 0;
         cuda_ok(cudaMemcpyAsync(lps_ctl(0), h.data(), sizeof(dev::Ctl) * n, cudaMemcpyHostToDevice, st), "ctl upload");
         cuda_ok(cudaMemsetAsync(B.next, 0, sizeof(unsigned), st), "memset");
         cuda_ok(cudaMemsetAsync(B.next_large, 0, sizeof(unsigned), st), "memset");
@@ -586,7 +586,7 @@ struct BatchImpl {
             cudaError_t q = cudaEventQuery(ev1);
             if (q == cudaSuccess) break;
             if (q != cudaErrorNotReady) cuda_ok(q, "batched kernel");
-            if (stop_flag && *stop_flag) *(volatile int*)h_stop = 1;
+            if (stop_requested(o, stop_flag)) *(volatile int*)h_stop = 1;
             std::this_thread::sleep_for(std::chrono::microseconds(20));
         }
         float ms = 0.0f;

@@ -201,6 +201,55 @@ int b2_server_submit_file(b2_server* s, const char* path, int64_t* ticket) {
     });
 }
 
+int b2_server_submit_lp(b2_server* s, const b2_lp_view* original, int32_t presolve, int64_t* ticket) {
+    return b2::guarded([&] {
+        if (!s || !original || !ticket) b2::fail(B2_ERR_INVALID, "null argument");
+        *ticket = b2::server_submit_lp(s->impl, *original, presolve != 0);
+    });
+}
+
+int b2_pdlp_form_build(const b2_lp_view* ranged, b2_pdlp_form** out) {
+    return b2::guarded([&] {
+        if (!ranged || !out) b2::fail(B2_ERR_INVALID, "null argument");
+        *out = reinterpret_cast<b2_pdlp_form*>(b2::pdlp_form_build(*ranged));
+    });
+}
+
+void b2_pdlp_form_view(const b2_pdlp_form* f, b2_lp_view* form) {
+    if (f && form) b2::pdlp_form_view(*reinterpret_cast<const b2::PdlpForm*>(f), *form);
+}
+
+int b2_pdlp_form_extract(const b2_pdlp_form* f, const double* x2, const double* y2, double* x, double* y) {
+    return b2::guarded([&] {
+        if (!f || !x2 || !y2 || !x || !y) b2::fail(B2_ERR_INVALID, "null argument");
+        b2::pdlp_form_extract(*reinterpret_cast<const b2::PdlpForm*>(f), x2, y2, x, y);
+    });
+}
+
+void b2_pdlp_form_destroy(b2_pdlp_form* f) { b2::pdlp_form_free(reinterpret_cast<b2::PdlpForm*>(f)); }
+
+int b2_presolve(const b2_lp_view* original, b2_presolved** out, int32_t* status) {
+    return b2::guarded([&] {
+        if (!original || !out) b2::fail(B2_ERR_INVALID, "null argument");
+        b2::Presolved* p = b2::presolve_lp(*original);
+        if (status) *status = b2::presolved_status(*p);
+        *out = reinterpret_cast<b2_presolved*>(p);
+    });
+}
+
+void b2_presolved_view(const b2_presolved* p, b2_lp_view* reduced) {
+    if (p && reduced) b2::presolved_view(*reinterpret_cast<const b2::Presolved*>(p), *reduced);
+}
+
+int b2_postsolve(const b2_presolved* p, const double* x_red, const double* y_red, double* x, double* y) {
+    return b2::guarded([&] {
+        if (!p || !x || !y) b2::fail(B2_ERR_INVALID, "null argument");
+        b2::postsolve_lp(*reinterpret_cast<const b2::Presolved*>(p), x_red, y_red, x, y);
+    });
+}
+
+void b2_presolved_destroy(b2_presolved* p) { b2::presolved_free(reinterpret_cast<b2::Presolved*>(p)); }
+
 int b2_lp_write(const char* path, const b2_lp_view* lp) {
     return b2::guarded([&] {
         if (!path || !lp) b2::fail(B2_ERR_INVALID, "null argument");

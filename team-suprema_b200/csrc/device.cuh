@@ -58,8 +58,9 @@ enum { MODE_START = 0, MODE_RESUME = 1, MODE_CONTINUE = 2 };
 // Group kinds: one CTA (barrier __syncthreads, partial sums in shared memory,
 // iterates read through L1), a thread-block cluster (hardware cluster
 // barrier), the whole grid of a cooperative launch (software grid barrier).
-// Across SMs, iterates and partial sums go through L2 (ld.global.cg). Every
-// barrier, of every kind, is preceded by a gpu-scope fence.
+// Across SMs, iterates and partial sums go through L2 (ld.global.cg); the
+// grid barrier fences once per CTA (thread 0, around its release/acquire), the
+// cluster barrier in every thread, the one-CTA barrier not at all.
 enum { GK_CTA = 0, GK_CLUSTER = 1, GK_GRID = 2 };
 // one record per KKT check: attempts, accepted, eps_P/D/G of the current point,
 // eps_P/D/G of the average, omega, eta, flags (restart | avg<<1 | fp32<<2 |
@@ -234,26 +235,32 @@ __device__ __forceinline__ double warp_total(double v) {
 // leaves.
 template <int GK>
 __device__ __forceinline__ bool group_sync(const Group& g) {
-    // Make this thread's stores visible at gpu scope before anyone crosses the
-    // barrier. Needed even inside one CTA: in testing on B200, iterates read
-    // after a bare __syncthreads (plain or L2 loads) were sometimes the values
-    // from before the other threads' stores, and the solve diverged.
-    __threadfence();
     if (GK == GK_CTA) {
+        // one CTA: bar.sync orders every thread's global and shared stores
+        // before the other threads' loads after it (CTA scope), and the
+        // iterates are read with plain (L1-coherent within the SM) loads
         __syncthreads();
         return true;
     }
     if (GK == GK_CLUSTER) {
+        // the hardware cluster barrier has no timeout, so every thread also
+        // fences its own stores at gpu scope first: a CTA of the cluster must
+        // never decide from a value it cannot yet see
+        __threadfence();
         asm volatile("barrier.cluster.arrive.release.aligned;\n\tbarrier.cluster.wait.acquire.aligned;" ::: "memory");
         return true;
     }
     __shared__ int s_ok;
+    // bar.sync makes the CTA's stores observed by thread 0; its gpu-scope
+    // fence and release then publish them cumulatively to the other CTAs,
+    // which read them at L2 (ld.global.cg) after their acquire and bar.sync
     __syncthreads();
     if (g.size == 1) return true;
     if (threadIdx.x == 0) {
         int ok = 1;
         const unsigned add = g.rank == 0 ? (0x80000000u - (unsigned)(g.size - 1)) : 1u;
         unsigned old;
+        __threadfence();
         asm volatile("atom.add.release.gpu.u32 %0,[%1],%2;" : "=r"(old) : "l"(g.bar), "r"(add) : "memory");
         const unsigned long long t0 = gtimer();
         unsigned spins = 0;
@@ -267,6 +274,7 @@ __device__ __forceinline__ bool group_sync(const Group& g) {
             }
         }
         if (ok && *(volatile int*)g.abort) ok = 0;
+        __threadfence();
         s_ok = ok;
     }
     __syncthreads();

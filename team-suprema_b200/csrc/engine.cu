@@ -346,7 +346,7 @@ struct EngineImpl {
         h.best_merit = std::numeric_limits<double>::infinity();
         h.xi = 0; h.yi = 0; h.ax_cur = 0; h.ax_nxt = 1; h.ax_avg = 2; h.aty_cur = 0; h.aty_avg = 1;
         h.mode = dev::MODE_START;
-        *h_stop = stop_flag ? *stop_flag : 0;
+        *h_stop = stop_requested(o, stop_flag) ? 1 : 0;
         cuda_ok(cudaMemcpyAsync(ctl, &h, sizeof(h), cudaMemcpyHostToDevice, st), "ctl upload");
         const int ctas = pick_ctas(o);
         const bool mixed = o.precision == B2_PREC_MIXED;
@@ -357,7 +357,7 @@ struct EngineImpl {
             auto P = params<float>(o, itf);
             launch<float, float>(P, ga, ctas, st);
             cuda_ok(cudaEventRecord(ev1, st), "event");
-            wait(stop_flag);
+            wait(o, stop_flag);
             dev::Ctl back{};
             cuda_ok(cudaMemcpy(&back, ctl, sizeof(back), cudaMemcpyDeviceToHost), "ctl download");
             check_abort();
@@ -372,7 +372,7 @@ struct EngineImpl {
                 if (exact) launch<double, float>(Q, ga, ctas, st);
                 else launch<double, double>(Q, ga, ctas, st);
                 cuda_ok(cudaEventRecord(ev1, st), "event");
-                wait(stop_flag);
+                wait(o, stop_flag);
                 check_abort();
             }
         } else {
@@ -380,7 +380,7 @@ struct EngineImpl {
             if (exact) launch<double, float>(Q, ga, ctas, st);
             else launch<double, double>(Q, ga, ctas, st);
             cuda_ok(cudaEventRecord(ev1, st), "event");
-            wait(stop_flag);
+            wait(o, stop_flag);
             check_abort();
         }
         float ms = 0.0f;
@@ -490,13 +490,13 @@ struct EngineImpl {
     }
 
     // Waits for the persistent kernel while mirroring the caller's stop flag
-    // into the mapped word the device polls.
-    void wait(const volatile int32_t* stop_flag) {
+    // (or stop callback) into the mapped word the device polls.
+    void wait(const b2_solve_opts& o, const volatile int32_t* stop_flag) {
         for (;;) {
             cudaError_t q = cudaEventQuery(ev1);
             if (q == cudaSuccess) return;
             if (q != cudaErrorNotReady) cuda_ok(q, "persistent kernel");
-            if (stop_flag && *stop_flag) *(volatile int*)h_stop = 1;
+            if (stop_requested(o, stop_flag)) *(volatile int*)h_stop = 1;
             struct timespec ts{0, 20000};
             nanosleep(&ts, nullptr);
         }

@@ -17,6 +17,13 @@ struct Error {
 [[noreturn]] void fail(int code, const std::string& msg);
 void set_last_error(const std::string& msg);
 
+// Whether the caller asked a running solve to stop: its stop word or its
+// stop callback (b2_solve_opts::stop_poll).
+inline bool stop_requested(const b2_solve_opts& o, const volatile int32_t* stop_flag) {
+    if (stop_flag && *stop_flag) return true;
+    return o.stop_poll && o.stop_poll(o.stop_ctx) != 0;
+}
+
 // Sliced ELL with a per-slice lane count ("lanes per row", g = 1..32).
 //
 // A slice is one warp's unit of work: 32/g consecutive rows (in the permuted
@@ -104,6 +111,21 @@ struct LpArrays {
     double obj_offset = 0.0;
 };
 
+// Presolve, PDLP form and postsolve (presolve.cpp). Throw Error.
+struct Presolved;
+struct PdlpForm;
+Presolved* presolve_lp(const b2_lp_view& original);
+int32_t presolved_status(const Presolved& p);  // 0 reduced, 1 infeasible, 2 unbounded
+void presolved_view(const Presolved& p, b2_lp_view& reduced);
+void postsolve_lp(const Presolved& p, const double* x_red, const double* y_red, double* x, double* y);
+void presolved_free(Presolved* p);
+PdlpForm* pdlp_form_build(const b2_lp_view& ranged);
+void pdlp_form_view(const PdlpForm& f, b2_lp_view& form);
+void pdlp_form_extract(const PdlpForm& f, const double* x2, const double* y2, double* x, double* y);
+void pdlp_form_free(PdlpForm* f);
+// verify()'s figures on the host: out = {eps_P, eps_D, eps_G, objective}
+void kkt_host(const b2_lp_view& lp, const double* x, const double* y, double* out);
+
 // The binary request format (lp_io.cpp). All functions throw Error.
 void lp_write(const std::string& path, const b2_lp_view& lp);
 void lp_read_dims(const std::string& path, int32_t* m, int32_t* n, int64_t* nnz);
@@ -149,6 +171,7 @@ ServerImpl* server_create(const b2_server_opts& so, const b2_solve_opts& o);
 void server_destroy(ServerImpl* s);
 int64_t server_submit(ServerImpl* s, const b2_lp_view& U);
 int64_t server_submit_file(ServerImpl* s, const std::string& path);
+int64_t server_submit_lp(ServerImpl* s, const b2_lp_view& original, bool presolve);
 int server_wait(ServerImpl* s, int64_t ticket, double timeout_s, double* x, double* y, b2_result* res,
                 b2_request_info* info);
 void server_stats(ServerImpl* s, b2_server_stats* out);

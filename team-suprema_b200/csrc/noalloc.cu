@@ -3,17 +3,19 @@
 // best point, control state, outputs) carved out of one file-scope static
 // __device__ array, so the call allocates no device memory.
 //
-// For callers that cannot call cudaMalloc: code that runs while a CUDA stream
-// is being captured into a graph (allocation is not a capturable stream
-// operation), processes whose GPU memory is handed out by a pool they do not
-// own, and real-time paths that must not enter the driver's allocator.
+// For callers that cannot call cudaMalloc: processes whose GPU memory is
+// reserved up front by another runtime's allocator or a pool they do not own
+// (a cudaMalloc from here would fail or fragment it), and latency-critical
+// paths that must stay out of the driver's allocator.
 //
 // Limits and sharing:
 //   * the array holds kNoAllocBytes (32 MiB): the layout, vectors and
 //     iterates of LPs up to roughly 200,000 nonzeros; larger LPs are rejected
 //     with B2_ERR_UNSUPPORTED before any GPU work;
-//   * every GPU that loads the library holds the array until the process
-//     exits;
+//   * when a device holds the array: with lazy module loading (CUDA's default
+//     since 12.2) from the first call on that device (its
+//     cudaGetSymbolAddress loads this file's module) until the process exits;
+//     with eager loading, on every device from library load;
 //   * every call in the process shares the one array and leaves its contents
 //     behind; whatever must start at zero is cleared by each call. Calls are
 //     serialized by a process-wide lock and each returns only after its GPU
@@ -21,7 +23,8 @@
 //     array;
 //   * the first call on a device looks up the array's device address
 //     (cudaGetSymbolAddress) with that device current; make that first call
-//     before any stream capture begins.
+//     before any stream capture begins;
+//   * the work runs on the legacy default stream, with synchronous copies.
 // Host memory is still used to build the sliced layout before it is copied
 // into the array.
 #include <algorithm>

@@ -6,8 +6,10 @@
 // restarted PDLP as one b2_batch LP (device.cuh, solve_body over one CTA), so
 // its answer does not depend on what else is in flight.
 //
-//   submit ──> prep threads: Ruiz + Pock-Chambolle scaling (src/scaling.cpp:25-84
-//              restated in host_prep.cpp), sliced layout, the LP's device image
+//   submit ──> prep threads: [an LP submitted as the caller has it: presolve
+//              and PDLP form (presolve.cpp)], Ruiz + Pock-Chambolle scaling
+//              (src/scaling.cpp:25-84 restated in host_prep.cpp), sliced
+//              layout, the LP's device image
 //          ──> admission, oldest first, while the LP's device footprint fits
 //              the HBM budget and a descriptor slot is free: one device region
 //              per LP (stream-ordered allocation) holding its matrix, vectors,
@@ -19,7 +21,10 @@
 //              left in the LP's region; the next round picks every LP up
 //              exactly where it stopped (MODE_CONTINUE), new arrivals join it
 //          ──> an LP whose exit reason is set is finished: its point and
-//              control state are copied out, its region freed, the caller woken.
+//              control state are copied out, its region freed, the caller woken;
+//              an LP submitted as the caller has it is mapped back (extract,
+//              postsolve) and its KKT figures taken on the original LP, on the
+//              waiting caller's thread.
 //
 // LPs with at least grid_nnz nonzeros take the whole-GPU lane instead: the
 // cooperative one-LP engine (engine.cu) runs them one at a time in slices of
@@ -172,6 +177,12 @@ enum ReqState { RQ_SUBMITTED = 0, RQ_PREPARED = 1, RQ_RESIDENT = 2, RQ_DONE = 3 
 struct Request {
     int64_t ticket = 0;
     std::string path;  // a request file, read on a preparation thread
+    // b2_server_submit_lp: the LP as the caller has it, its presolve and its
+    // PDLP form; the fields below then hold the PDLP form
+    bool ranged = false, do_presolve = false, trivial = false;
+    LpArrays orig;
+    std::unique_ptr<Presolved, void (*)(Presolved*)> pre{nullptr, presolved_free};
+    std::unique_ptr<PdlpForm, void (*)(PdlpForm*)> form{nullptr, pdlp_form_free};
     // the LP as submitted (unscaled PDLP form)
     int32_t m = 0, n = 0;
     std::vector<int32_t> row, col;
@@ -386,6 +397,96 @@ struct ServerImpl {
         return enqueue(std::move(r));
     }
 
+    int64_t submit_lp(const b2_lp_view& O, bool presolve) {
+        if (O.m < 0 || O.n < 0 || O.nnz < 0) fail(B2_ERR_INVALID, "negative size");
+        if (O.nnz > 0 && (!O.row_idx || !O.col_idx || !O.val)) fail(B2_ERR_INVALID, "null matrix arrays");
+        if ((O.n > 0 && (!O.c || !O.l || !O.u)) || (O.m > 0 && (!O.rL || !O.rU))) fail(B2_ERR_INVALID, "null vectors");
+        std::unique_ptr<Request> r(new Request());
+        r->ranged = true;
+        r->do_presolve = presolve;
+        LpArrays& a = r->orig;
+        a.m = O.m;
+        a.n = O.n;
+        a.row.assign(O.row_idx, O.row_idx + O.nnz);
+        a.col.assign(O.col_idx, O.col_idx + O.nnz);
+        a.val.assign(O.val, O.val + O.nnz);
+        a.c.assign(O.c, O.c + O.n);
+        a.l.assign(O.l, O.l + O.n);
+        a.u.assign(O.u, O.u + O.n);
+        a.rL.assign(O.rL, O.rL + O.m);
+        a.rU.assign(O.rU, O.rU + O.m);
+        a.obj_offset = O.obj_offset;
+        r->work = request_work(O.m, O.n, O.nnz);
+        return enqueue(std::move(r));
+    }
+
+    static b2_lp_view view_of(const LpArrays& a) {
+        return b2_lp_view{a.m, a.n, (int64_t)a.val.size(), a.row.data(), a.col.data(), a.val.data(), a.c.data(),
+                          a.rL.data(), a.rU.data(), a.l.data(), a.u.data(), a.obj_offset};
+    }
+
+    // The caller's LP -> [presolve] -> PDLP form, into the request's form
+    // fields (src/solve.cpp:150-195 does the same before its PDLP stage).
+    void to_pdlp_form(Request& r) {
+        const b2_lp_view O = view_of(r.orig);
+        b2_lp_view src = O;
+        if (r.do_presolve) {
+            r.pre.reset(presolve_lp(O));
+            const int32_t st = presolved_status(*r.pre);
+            if (st == 1) fail(B2_ERR_INFEASIBLE, "presolve: the LP is infeasible");
+            if (st == 2) fail(B2_ERR_UNBOUNDED, "presolve: the LP is unbounded");
+            presolved_view(*r.pre, src);
+        }
+        if (src.m == 0 || src.n == 0) {
+            if (!r.do_presolve) fail(B2_ERR_INVALID, "an LP with no rows or no columns needs presolve");
+            r.trivial = true;  // presolve solved it: no GPU work
+            return;
+        }
+        r.form.reset(pdlp_form_build(src));
+        b2_lp_view F;
+        pdlp_form_view(*r.form, F);
+        r.m = F.m;
+        r.n = F.n;
+        r.row.assign(F.row_idx, F.row_idx + F.nnz);
+        r.col.assign(F.col_idx, F.col_idx + F.nnz);
+        r.val.assign(F.val, F.val + F.nnz);
+        r.c.assign(F.c, F.c + F.n);
+        r.l.assign(F.l, F.l + F.n);
+        r.u.assign(F.u, F.u + F.n);
+        r.rL.assign(F.rL, F.rL + F.m);
+        r.rU.assign(F.rU, F.rU + F.m);
+        r.obj_offset = F.obj_offset;
+    }
+
+    // The PDLP-form answer of a ranged request -> the caller's LP, and
+    // verify()'s figures there. Runs on the waiting caller's thread.
+    void map_back(Request& r, std::vector<double>& x0, std::vector<double>& y0, b2_request_info* info) {
+        const b2_lp_view O = view_of(r.orig);
+        x0.assign(std::max(O.n, 1), 0.0);
+        y0.assign(std::max(O.m, 1), 0.0);
+        std::vector<double> xr, yr;
+        b2_lp_view red = O;
+        if (r.pre) presolved_view(*r.pre, red);
+        xr.assign(std::max(red.n, 1), 0.0);
+        yr.assign(std::max(red.m, 1), 0.0);
+        if (r.form) pdlp_form_extract(*r.form, r.x.data(), r.y.data(), xr.data(), yr.data());
+        if (r.pre) postsolve_lp(*r.pre, xr.data(), yr.data(), x0.data(), y0.data());
+        else { x0 = xr; y0 = yr; }
+        if (info) {
+            info->form_eps[0] = r.res.eps_P;
+            info->form_eps[1] = r.res.eps_D;
+            info->form_eps[2] = r.res.eps_G;
+            info->presolved_m = r.form ? r.m : 0;
+            info->presolved_n = r.form ? r.n : 0;
+        }
+        double k[4];
+        kkt_host(O, x0.data(), y0.data(), k);
+        r.res.eps_P = k[0];
+        r.res.eps_D = k[1];
+        r.res.eps_G = k[2];
+        r.res.objective = k[3];
+    }
+
     int64_t submit_file(const std::string& path) {
         std::unique_ptr<Request> r(new Request());
         r->path = path;
@@ -439,6 +540,20 @@ struct ServerImpl {
                 continue;
             }
             r->prep_ms = std::chrono::duration<double, std::milli>(Clock::now() - t0).count();
+            if (r->trivial) {  // presolve left nothing to solve
+                std::memset(&r->res, 0, sizeof(r->res));
+                r->res.converged = 1;
+                r->res.exit_reason = B2_EXIT_CONVERGED;
+                {
+                    std::lock_guard<std::mutex> lk(mu);
+                    r->state = RQ_DONE;
+                    st.backlog_work -= r->work;
+                    r->t_prepared = r->t_admit = r->t_done = now_s();
+                    st.completed++;
+                }
+                cv_done.notify_all();
+                continue;
+            }
             {
                 std::lock_guard<std::mutex> lk(mu);
                 r->state = RQ_PREPARED;
@@ -452,6 +567,10 @@ struct ServerImpl {
     // Scaling (src/scaling.cpp:25-84, 10 Ruiz passes + Pock-Chambolle) and the
     // device layout; the batched lane also gets its region plan and image.
     void prepare(Request& r) {
+        if (r.ranged) {
+            to_pdlp_form(r);
+            if (r.trivial) return;
+        }
         if (!r.path.empty()) {
             LpArrays a;
             lp_read(r.path, a);
@@ -843,14 +962,21 @@ struct ServerImpl {
         }
         const int err = r->err;
         const std::string msg = r->err_msg;
-        if (!err) {
+        reqs.erase(it);
+        lk.unlock();
+        // the request is the caller's alone now
+        std::unique_ptr<Request> own(r);
+        if (err) fail(err, msg);
+        if (r->ranged) {
+            std::vector<double> x0, y0;
+            map_back(*r, x0, y0, info);
+            if (x && r->orig.n) std::memcpy(x, x0.data(), sizeof(double) * r->orig.n);
+            if (y && r->orig.m) std::memcpy(y, y0.data(), sizeof(double) * r->orig.m);
+        } else {
             if (x && r->n) std::memcpy(x, r->x.data(), sizeof(double) * r->n);
             if (y && r->m) std::memcpy(y, r->y.data(), sizeof(double) * r->m);
-            if (res) *res = r->res;
         }
-        reqs.erase(it);
-        delete r;
-        if (err) fail(err, msg);
+        if (res) *res = r->res;
         return B2_OK;
     }
 
@@ -872,6 +998,7 @@ ServerImpl* server_create(const b2_server_opts& so, const b2_solve_opts& o) {
 void server_destroy(ServerImpl* s) { delete s; }
 int64_t server_submit(ServerImpl* s, const b2_lp_view& U) { return s->submit(U); }
 int64_t server_submit_file(ServerImpl* s, const std::string& path) { return s->submit_file(path); }
+int64_t server_submit_lp(ServerImpl* s, const b2_lp_view& O, bool presolve) { return s->submit_lp(O, presolve); }
 int server_wait(ServerImpl* s, int64_t ticket, double timeout_s, double* x, double* y, b2_result* res,
                 b2_request_info* info) {
     return s->wait(ticket, timeout_s, x, y, res, info);

@@ -16,11 +16,9 @@
 //   * errors are thrown as std::runtime_error (gpu/pdlp_gpu_solve.cu:32-38),
 //     which every caller catches on its own thread (src/solve.cpp:108-122).
 #include <atomic>
-#include <chrono>
 #include <cstdint>
 #include <stdexcept>
 #include <string>
-#include <thread>
 #include <vector>
 
 #include "b200_pdlp.h"
@@ -45,6 +43,12 @@ b2_lp_view view_of(const RangedLP& r) {
     return v;
 }
 
+// The engine's wait loop calls this about every 20 us while the solve runs:
+// a relaxed load of the caller's flag, as include/pdlp.hpp:30-34 polls it.
+int32_t poll_stop(void* ctx) {
+    return static_cast<const std::atomic<bool>*>(ctx)->load(std::memory_order_relaxed) ? 1 : 0;
+}
+
 }  // namespace
 
 PdlpResult solve_pdhg_gpu(const RangedLP& unscaled_form, const RangedLP& scaled_form, const std::vector<double>& Dr,
@@ -53,28 +57,21 @@ PdlpResult solve_pdhg_gpu(const RangedLP& unscaled_form, const RangedLP& scaled_
     const b2_lp_view U = view_of(unscaled_form), S = view_of(scaled_form);
     if ((int)Dr.size() != U.m || (int)Dc.size() != U.n)
         throw std::runtime_error("solve_pdhg_gpu: Dr/Dc sizes do not match the PDLP form");
-    // The device polls a plain int word; mirror the caller's atomic into it
-    // while the solve runs.
-    volatile int32_t stop_word = 0;
-    std::atomic<bool> done{false};
-    std::thread mirror;
+    b2_solve_opts o;
+    b2_default_opts(&o);
+    o.max_iterations = max_iterations;
+    o.check_every = check_every;
+    o.tol = tol;
     if (stop_flag) {
-        stop_word = stop_flag->load(std::memory_order_relaxed) ? 1 : 0;
-        mirror = std::thread([&]() {
-            while (!done.load(std::memory_order_relaxed)) {
-                if (stop_flag->load(std::memory_order_relaxed)) stop_word = 1;
-                std::this_thread::sleep_for(std::chrono::microseconds(100));
-            }
-        });
+        o.stop_poll = poll_stop;
+        o.stop_ctx = stop_flag;
     }
+    (void)eta;  // adaptive step size (gpu/pdlp_gpu_solve.cu:263)
     PdlpResult res;
     res.x.assign(U.n, 0.0);
     res.y.assign(U.m, 0.0);
     b2_result r{};
-    const int rc = b2_solve_pdhg_gpu(&U, &S, Dr.data(), Dc.data(), eta, max_iterations, check_every, tol,
-                                     stop_flag ? &stop_word : nullptr, res.x.data(), res.y.data(), &r);
-    done.store(true);
-    if (mirror.joinable()) mirror.join();
+    const int rc = b2_solve_pdhg_gpu_ex(&U, &S, Dr.data(), Dc.data(), &o, nullptr, res.x.data(), res.y.data(), &r);
     if (rc != B2_OK) throw std::runtime_error(std::string("b200 PDLP engine (code ") + std::to_string(rc) + "): " +
                                               b2_last_error());
     res.iterations = r.iterations;

@@ -70,6 +70,18 @@ def rel(a: float, b: float) -> float:
     return abs(a - b) / max(1.0, abs(b))
 
 
+OBJ_TOL = 1e-6
+
+
+def fixture_obj_tol(name: str) -> float:
+    """Objective bound of a fixture solved to 1e-6: 1e-6 relative, or twice the
+    reference PDLP's own gap to the dual simplex where that is larger (adlittle:
+    the reference's PDLP at 1e-6 lands 1.54e-6 from the simplex)."""
+    g = golden_index()["fixtures"][name]
+    own = rel(g["pdlp"]["1e-06"]["form_objective"], g["simplex"]["objective"])
+    return max(OBJ_TOL, 2.0 * own)
+
+
 @pytest.fixture(scope="session")
 def golden():
     return golden_index()

@@ -8,7 +8,7 @@ For every LP fixture the reference's own tests solve with PDLP
   * the PDLP-form problem exactly as solve_pdhg_gpu receives it -- presolve
     (src/presolve.cpp:524) -> build_pdlp_form (src/pdlp.cpp:8-82) -> scale
     (src/scaling.cpp:25-84): unscaled form, scaled values/vectors, Dr, Dc;
-and in ``golden.json``:
+in ``orig_<name>.npz`` the LP as read (to_ranged_lp, before presolve); and in ``golden.json``:
   * the reference CPU PDLP result on that form (solve_pdhg, src/pdlp.cpp:146) at
     tol 1e-6 and 1e-8: iterations, restarts, eps, the PDLP-form objective, and the
     original-space objective/eps after extract_solution + postsolve + verify;
@@ -70,10 +70,28 @@ def digest(lp) -> str:
     return h.hexdigest()[:16]
 
 
+def originals(ref: str):
+    """orig_<name>.npz: each fixture's LP as the reference reads it, before
+    presolve (read_mps -> to_ranged_lp, include/ranged_lp.hpp:39-62), for the
+    presolve and PDLP-form tests."""
+    for name in CASES + ["tiny_infeasible", "tiny_unbounded"]:
+        path = os.path.join(ref, "sample_problems", f"{name}.mps")
+        if not os.path.exists(path):
+            continue
+        P = O.RefProblem.from_mps(path, use_presolve=False)
+        f = P.form(P.ORIGINAL)
+        np.savez_compressed(os.path.join(HERE, f"orig_{name}.npz"), **form_arrays("o", f))
+        print("original", name, f.m, f.n, f.nnz)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--ref", default="/root/reference")
+    ap.add_argument("--originals", action="store_true", help="only write the orig_<name>.npz files")
     args = ap.parse_args()
+    if args.originals:
+        originals(args.ref)
+        return
     gold = {"fixtures": {}, "random": {}}
     for name in CASES:
         path = os.path.join(args.ref, "sample_problems", f"{name}.mps")
@@ -110,6 +128,7 @@ def main():
         print(key, gold["random"][key]["pdlp"]["1e-06"]["iterations"], spx["status"])
     with open(os.path.join(HERE, "golden.json"), "w") as f:
         json.dump(gold, f, indent=1, sort_keys=True, default=float)
+    originals(args.ref)
 
 
 if __name__ == "__main__":

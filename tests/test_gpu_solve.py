@@ -5,9 +5,11 @@ Every returned point is certified by the oracle's restated verify()
 numbers -- and its objective is compared with the reference CPU PDLP and the
 reference FP64 dual simplex on the same inputs (golden fixtures made by
 running the reference, tests/golden/make_golden.py). Tolerances:
-  * tol 1e-6: eps_P, eps_D, eps_G <= 1e-6 (certified), objective within 1e-5
-    relative of the dual simplex (the reference's own PDLP at 1e-6 lands within
-    1.5e-6 of it on these fixtures);
+  * tol 1e-6: eps_P, eps_D, eps_G <= 1e-6 (certified); the engine's own
+    eps_P/eps_D/eps_G agree with the independent check; objective within 1e-6
+    relative of the dual simplex and of the reference CPU PDLP at 1e-6. The one
+    exception is adlittle, where the reference's own PDLP at 1e-6 lands 1.54e-6
+    from the simplex: there both bounds are twice the reference's own gap;
   * tol 1e-8: objective within 1e-6 relative of the dual simplex and of the
     reference PDLP at 1e-8.
 """
@@ -16,7 +18,7 @@ import pytest
 
 import b200pdlp as B
 import oracle as O
-from conftest import as_form, fixture_names, golden_index, load_fixture, random_case, rel
+from conftest import OBJ_TOL, as_form, fixture_names, fixture_obj_tol, golden_index, load_fixture, random_case, rel
 
 pytestmark = pytest.mark.gpu
 
@@ -38,10 +40,15 @@ def test_fixture_tol_1e6(name, precision):
     assert r.converged, (r.iterations, r.eps_P, r.eps_D, r.eps_G)
     v, worst = certified(U, r, 1e-6)
     assert worst <= 1e-6 * (1 + 1e-9), v
-    # the engine's own report agrees with the independent check
+    # the engine's own report (its device-side KKT check) agrees with the independent check
     assert r.eps_P == pytest.approx(v["eps_P"], rel=1e-6, abs=1e-12)
-    assert rel(v["objective"], g["simplex"]["objective"]) <= 1e-5
-    assert rel(v["objective"], g["pdlp"]["1e-06"]["form_objective"]) <= 1e-5
+    assert r.eps_D == pytest.approx(v["eps_D"], rel=1e-6, abs=1e-12)
+    assert r.eps_G == pytest.approx(v["eps_G"], rel=1e-6, abs=1e-12)
+    tol_obj = fixture_obj_tol(name)
+    e_spx = rel(v["objective"], g["simplex"]["objective"])
+    e_ref = rel(v["objective"], g["pdlp"]["1e-06"]["form_objective"])
+    print(f"OBJ {name} prec={precision} vs_simplex={e_spx:.2e} vs_ref_pdlp={e_ref:.2e} bound={tol_obj:.2e}")
+    assert e_spx <= tol_obj and e_ref <= tol_obj, (e_spx, e_ref, tol_obj)
 
 
 @pytest.mark.parametrize("name", ["afiro", "sc50a", "blend", "beaconfd", "israel", "share1b"])
@@ -59,12 +66,18 @@ def test_fixture_tol_1e8(name):
 @pytest.mark.parametrize("key", sorted(G["random"].keys()))
 def test_random_family(key):
     lp, U, S, Dr, Dc, g = random_case(key)
-    for tol, obj_tol in ((1e-6, 1e-5), (1e-8, 1e-6)):
+    for tol in (1e-6, 1e-8):
         r = B.solve_pdhg_gpu(U, S, Dr, Dc, 0.99, 500000, 64, tol)
         assert r.converged
         v, worst = certified(U, r, tol)
         assert worst <= tol * (1 + 1e-6)
-        assert rel(v["objective"], g["simplex"]["objective"]) <= obj_tol
+        assert r.eps_P == pytest.approx(v["eps_P"], rel=1e-6, abs=1e-12)
+        assert r.eps_D == pytest.approx(v["eps_D"], rel=1e-6, abs=1e-12)
+        assert r.eps_G == pytest.approx(v["eps_G"], rel=1e-6, abs=1e-12)
+        e_spx = rel(v["objective"], g["simplex"]["objective"])
+        e_ref = rel(v["objective"], g["pdlp"][f"{tol:g}"]["form_objective"])
+        print(f"OBJ {key} tol={tol:g} vs_simplex={e_spx:.2e} vs_ref_pdlp={e_ref:.2e}")
+        assert e_spx <= OBJ_TOL and e_ref <= OBJ_TOL, (e_spx, e_ref)
 
 
 @pytest.mark.parametrize("name", ["afiro", "blend", "israel", "share1b"])
@@ -112,6 +125,28 @@ def test_stop_flag_before_start_returns_best_unconverged():
     assert np.all(np.isfinite(r.x)) and np.all(np.isfinite(r.y))
     v, _ = certified(U, r, 1e-6)
     assert r.eps_P == pytest.approx(v["eps_P"], rel=1e-6, abs=1e-12)
+
+
+def test_stop_callback_stops_a_running_solve():
+    """b2_solve_opts::stop_poll (what the shim passes for the reference's
+    std::atomic<bool> stop flag): polled by the waiting thread while the
+    persistent kernel runs; a nonzero answer stops it like stop_flag."""
+    import ctypes as C
+    lp = B.gen_random_lp(20_000, 60_000, 6, 7, True)
+    U, S, Dr, Dc, _ = B.prepare(lp)
+    calls = [0]
+
+    @C.CFUNCTYPE(C.c_int32, C.c_void_p)
+    def poll(_ctx):
+        calls[0] += 1
+        return 1 if calls[0] > 50 else 0
+
+    r = B.solve_pdhg_gpu(U, S, Dr, Dc, 0.99, 10_000_000, 64, 1e-12, precision=B.PREC_FP64,
+                         stop_poll=C.cast(poll, C.c_void_p).value)
+    assert not r.converged
+    assert r.stats["exit_reason"] == B.EXIT_STOPPED
+    assert calls[0] > 50
+    assert np.all(np.isfinite(r.x)) and np.all(np.isfinite(r.y))
 
 
 def test_iteration_limit_reports_best_point():
@@ -171,7 +206,8 @@ def test_inequality_rows_and_free_columns():
         v, worst = certified(U, r, 1e-7)
         assert worst <= 1e-7 * (1 + 1e-6)
         vr = O.verify(as_form(U), ref["x"], ref["y"])
-        assert rel(v["objective"], vr["objective"]) <= 1e-5
+        # both points within 1e-7 KKT of the same optimum
+        assert rel(v["objective"], vr["objective"]) <= OBJ_TOL
 
 
 def test_transport_split_layout_solve_certified():
@@ -189,7 +225,7 @@ def test_transport_split_layout_solve_certified():
     assert res[0]["converged"]
     v2 = O.verify(as_form(U), x, y)
     assert max(v2["eps_P"], v2["eps_D"], v2["eps_G"]) <= 1e-6 * (1 + 1e-9)
-    assert rel(v["objective"], v2["objective"]) <= 1e-5
+    assert rel(v["objective"], v2["objective"]) <= OBJ_TOL
     # repeated solves on the split layout are bit-identical (fixed segment order)
     with B.Engine(U, S, Dr, Dc) as eng:
         a = eng.solve(max_iterations=3000, tol=1e-9)

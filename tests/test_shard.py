@@ -90,7 +90,7 @@ def _rank_main(rank, world, port, out):
     import bench
     import b200pdlp as B_
     w, r, _ = bench.dist_setup(world)
-    shapes = bench.batch_shapes(B_, "batch", 96, 0, w)
+    shapes = bench.batch_shapes("batch", 96, 0, w)
     batch = bench.my_share(B_, [B_.request_work(m, n, n * k) for (m, n, k, _) in shapes], w, r)
     full = bench.serve_stream(2000.0 * w, 0.05, 0)
     stream = bench.my_share(B_, [B_.request_work(m, n, n * k) for (_, m, n, k, _) in full], w, r, online=True)
@@ -111,7 +111,7 @@ def test_two_gloo_ranks_take_disjoint_covering_shares():
     assert sorted(s0 + s1) == list(range(ns)) and s0 and s1
     # the loads of the two batch shares are close (longest first)
     import bench
-    shapes = bench.batch_shapes(B, "batch", 96, 0, 2)
+    shapes = bench.batch_shapes("batch", 96, 0, 2)
     work = np.array([B.request_work(m, n, n * k) for (m, n, k, _) in shapes])
     l0, l1 = work[b0].sum(), work[b1].sum()
     assert abs(l0 - l1) <= work.max()
