@@ -698,6 +698,67 @@ def reference_many(args, world, rank):
             "steps_detail": stats}
 
 
+def other_configs(args, peak_gbs):
+    """The other benchmark configurations, measured after the headline LP on
+    one GPU so that every config has a number in the same run: the 2,000 x 500
+    transportation LP (K solves from HBM-resident data, CUDA events) and the
+    4,096-LP batch (one persistent launch per step). Each entry carries its
+    own clocks record."""
+    import torch
+    import b200pdlp as B
+    out = {}
+    prec = B.PREC_MIXED if args.precision == "mixed" else B.PREC_FP64
+    # transportation LP
+    lp = make_lp(B, "transport")
+    U, S, Dr, Dc, _ = B.prepare(lp)
+    stream = torch.cuda.Stream()
+    with B.Engine(U, S, Dr, Dc, precision=prec, stream=stream.cuda_stream) as eng:
+        def one():
+            return eng.solve(max_iterations=2_000_000, tol=args.tol, copy_out=False, precision=prec,
+                             stream=stream.cuda_stream)
+        for _ in range(3):
+            one()
+        torch.cuda.synchronize()
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+        res = []
+        with ClockSampler(torch.cuda.current_device()) as clk:
+            ev[0].record(stream)
+            for _ in range(args.extra_steps):
+                res.append(one())
+            ev[1].record(stream)
+            torch.cuda.synchronize()
+        ms = ev[0].elapsed_time(ev[1])
+        m, n, z = U.m, U.n, U.nnz
+        tot_b = sum(r.stats["fp32_accepted"] * algorithmic_bytes(m, n, z, 4)
+                    + (r.stats["accepted"] - r.stats["fp32_accepted"]) * algorithmic_bytes(m, n, z, 8) for r in res)
+        dev_ms = sum(r.stats["device_ms"] for r in res)
+        a_ms = eng.spmv_bench(0, B.PREC_MIXED, 50, stream.cuda_stream)
+        r0 = res[-1]
+        out["transport"] = {
+            "workload": describe("transport"), "value": args.extra_steps / (ms / 1e3), "unit": UNIT,
+            "ms_per_step": ms / args.extra_steps, "steps": args.extra_steps, "warmup": 3,
+            "attempts": r0.iterations, "fp32_attempts": r0.stats["fp32_attempts"], "converged": r0.converged,
+            "eps": [r0.eps_P, r0.eps_D, r0.eps_G],
+            "roofline": {"bound": "hbm", "achieved": tot_b / (dev_ms / 1e3) / 1e9, "peak": peak_gbs, "unit": "GB/s",
+                         "frac": tot_b / (dev_ms / 1e3) / 1e9 / peak_gbs, "kernel": "k_pdlp (persistent solve)"},
+            "spmv_A_frac": spmv_bytes(m, n, z) / (a_ms / 1e3) / 1e9 / peak_gbs, "clocks": clk.summary()}
+    # the uneven batch
+    probs, n_total = make_batch(B, "batch")
+    with B.Batch(probs) as bt:
+        info = bt.info()
+        bt.solve(max_iterations=2_000_000, tol=args.tol, precision=prec)
+        with ClockSampler(torch.cuda.current_device()) as clk:
+            res, ms = bt.solve(max_iterations=2_000_000, tol=args.tol, precision=prec)
+        lat = sorted(r["device_ms"] for r in res)
+        out["batch"] = {
+            "workload": describe("batch"), "value": n_total / (ms / 1e3), "unit": UNIT, "ms_per_step": ms,
+            "steps": 1, "warmup": 1, "converged": int(sum(r["converged"] for r in res)), "lps": n_total,
+            "latency_ms": {"p50": lat[len(lat) // 2], "p99": lat[int(0.99 * (len(lat) - 1))], "max": lat[-1],
+                           "note": "per-LP time on its CTA inside the launch"},
+            "sum_nnz": info["sum_nnz"], "clocks": clk.summary()}
+    return out
+
+
 def profile_mode(args):
     """Short runs for profiler captures: builds the engine for the workload and
     launches only the kernel under study."""
@@ -729,6 +790,9 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=2)
     ap.add_argument("--cpu-sample-iters", type=int, default=40)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-other-configs", action="store_true",
+                    help="large LP: skip the transport LP and batch measurements added to the line")
+    ap.add_argument("--extra-steps", type=int, default=5, help="timed solves of the transport LP in other_configs")
     ap.add_argument("--cpu-budget-s", type=float, default=15.0,
                     help="batch / serve: wall seconds of the all-cores reference CPU sample (per step)")
     ap.add_argument("--mode", default="bench", choices=["bench", "spmv", "solve"],
@@ -856,6 +920,10 @@ def main():
         except Exception as e:  # the baseline is reported, not required
             cpu = {"error": str(e)}
 
+    others = None
+    if rank == 0 and world == 1 and args.workload == "large" and not args.no_other_configs:
+        others = other_configs(args, peak_gbs)
+
     if rank == 0:
         clocks = clk.summary()
         r0 = results[-1]
@@ -883,6 +951,7 @@ def main():
                     "ms_per_step": statistics.mean(e2e_ms)},
             "cpu_baseline": cpu, "clocks": clocks, "gpu_launches": launches,
             "prep_s": t_prep, "layout": {k: info[k] for k in ("ctas", "a_padded", "at_padded", "values_exact_fp32")},
+            "other_configs": others,
         }
         print(json.dumps(line), flush=True)
     eng.close()
