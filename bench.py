@@ -470,6 +470,8 @@ def batch_bench(args, world, rank, local):
     value = n_total * args.steps / (ms_total / 1e3)
     res = steps[-1][0]
     lat = sorted(r["device_ms"] for r in res)
+    lp_cta_ms = float(sum(r["device_ms"] * max(1, r["group_ctas"]) for r in res))
+    launch_ctas = bt.info()["last_launch_ctas"]
     conv = int(dist_sum(sum(r["converged"] for r in res), world))
     attempts = np.array([r["iterations"] for r in res])
     cpu = None
@@ -495,9 +497,10 @@ def batch_bench(args, world, rank, local):
                        else "single GPU"},
             "latency_ms": {"p50": lat[len(lat) // 2], "p99": lat[int(0.99 * (len(lat) - 1))], "max": lat[-1],
                            "note": "per-LP time on its CTA inside the launch (rank 0's share)"},
-            "occupancy": {"lp_ms_sum": float(sum(lat)), "ctas": info["max_ctas"],
-                          "busy_fraction": float(sum(lat)) / (steps[-1][1] * max(1, info["max_ctas"])),
-                          "note": "sum of the LPs' times on their CTAs over (launch time x CTAs), last step"},
+            "occupancy": {"lp_cta_ms": lp_cta_ms, "ctas": launch_ctas,
+                          "busy_fraction": lp_cta_ms / (steps[-1][1] * max(1, launch_ctas)),
+                          "note": "sum over LPs of (time on its CTAs x CTAs in its group) over (launch time x "
+                                  "CTAs the launch used), last step"},
             "converged": conv, "attempts": {"median": float(np.median(attempts)), "max": int(attempts.max()),
                                             "total": int(attempts.sum())},
             "clocks": clk.summary(), "gpu_launches": args.steps, "prep_s": t_prep, "create_s": t_create,
@@ -772,7 +775,8 @@ def profile_mode(args):
             t = eng.spmv_bench(1, prec, args.reps)
             print(f"spmv A {a * 1e3:.1f} us, A^T {t * 1e3:.1f} us ({args.precision} vectors)")
         else:
-            r = eng.solve(max_iterations=args.max_attempts, tol=args.tol, precision=prec, copy_out=False)
+            extra = {"switch_tol": args.switch_tol} if args.switch_tol > 0 else {}
+            r = eng.solve(max_iterations=args.max_attempts, tol=args.tol, precision=prec, copy_out=False, **extra)
             print(f"solve: {r.iterations} attempts ({r.stats['fp32_attempts']} FP32), "
                   f"{r.stats['device_ms']:.2f} ms, {1e3 * r.stats['device_ms'] / max(1, r.iterations):.1f} us/attempt, "
                   f"tol {args.tol:g}, converged {r.converged}, eps {r.eps_P:.3e} {r.eps_D:.3e} {r.eps_G:.3e}")
@@ -798,6 +802,8 @@ def main():
     ap.add_argument("--mode", default="bench", choices=["bench", "spmv", "solve"],
                     help="spmv / solve: one short run of that kernel for profiling (ncu), no JSON line")
     ap.add_argument("--max-attempts", type=int, default=256, help="--mode solve: attempt limit")
+    ap.add_argument("--switch-tol", type=float, default=0.0,
+                    help="--mode solve, mixed precision: KKT level of the FP32 -> FP64 hand-over (0: default)")
     ap.add_argument("--reps", type=int, default=1, help="--mode spmv: timed launches per product")
     ap.add_argument("--batch-block", type=int, default=0, help="batch: threads per CTA (128/256/512, 0 auto)")
     ap.add_argument("--batch-count", type=int, default=0, help="batch: LPs (0: 4096)")

@@ -288,6 +288,8 @@ struct PoolOffsets {
 
 struct BatchImpl {
     int n = 0, sm_count = 0, max_ctas = 0, last_nt = 256;
+    int last_ctas = 0;               // CTAs of the last launch (both lanes)
+    std::vector<char> last_cluster;  // per LP: solved by a cluster in the last launch
     BatchShape shape{};
     cudaStream_t stream = nullptr, stream2 = nullptr;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr, ev_small = nullptr;
@@ -531,9 +533,14 @@ struct BatchImpl {
         const int ntx = batch_nt_index(nt);
         last_nt = nt;
         std::vector<int> small_q, large_q;
+        last_cluster.assign(n, 0);
         for (int i : order) {
-            if (shape.max_clusters_nt[ntx] > 0 && L[i].A.padded + L[i].AT.padded >= big) large_q.push_back(i);
-            else small_q.push_back(i);
+            if (shape.max_clusters_nt[ntx] > 0 && L[i].A.padded + L[i].AT.padded >= big) {
+                large_q.push_back(i);
+                last_cluster[i] = 1;
+            } else {
+                small_q.push_back(i);
+            }
         }
         if (o.max_iterations < 0) fail(B2_ERR_INVALID, "max_iterations < 0");
         std::vector<dev::Ctl> h(n);
@@ -567,6 +574,7 @@ struct BatchImpl {
             int ncl = std::min((int)large_q.size(), std::max(1, shape.max_clusters_nt[ntx] / 2));
             if (o.max_ctas > 0) ncl = std::max(1, std::min(ncl, o.max_ctas / dev::kMaxCluster));
             batch_kernel_launch(B, true, nt, ncl, st);
+            last_ctas = ncl * dev::kMaxCluster;
             const int rest = (o.max_ctas > 0 ? std::min(o.max_ctas, shape.max_ctas_nt[ntx]) : shape.max_ctas_nt[ntx]) -
                              ncl * dev::kMaxCluster;
             if (!small_q.empty() && rest > 0) {
@@ -574,12 +582,14 @@ struct BatchImpl {
                 dev::BatchArgs Bs = B;
                 Bs.n_large = 0;
                 batch_kernel_launch(Bs, false, nt, std::min(rest, (int)small_q.size()), stream2);
+                last_ctas += std::min(rest, (int)small_q.size());
                 cuda_ok(cudaEventRecord(ev_small, stream2), "event");
                 cuda_ok(cudaStreamWaitEvent(st, ev_small, 0), "wait");
             }
         } else {
             const int ctas = std::max(1, std::min(shape.max_ctas_nt[ntx], o.max_ctas > 0 ? std::min(o.max_ctas, n) : n));
             batch_kernel_launch(B, false, nt, ctas, st);
+            last_ctas = ctas;
         }
         cuda_ok(cudaEventRecord(ev1, st), "event");
         for (;;) {
@@ -602,6 +612,7 @@ struct BatchImpl {
                 fill_result(last_ctl[i], res[i]);
                 res[i].device_ms = (double)(t1[i] - t0[i]) * 1e-6;
                 res[i].objective = std::numeric_limits<double>::quiet_NaN();
+                res[i].group_ctas = last_cluster[i] ? dev::kMaxCluster : 1;
             }
         }
     }
@@ -635,6 +646,7 @@ struct BatchImpl {
         inf->max_ctas = max_ctas;
         inf->threads_per_cta = last_nt;
         inf->device_bytes = (int64_t)bytes;
+        inf->last_launch_ctas = last_ctas;
     }
 };
 

@@ -272,6 +272,7 @@ void solve_noalloc(const b2_lp_view& U, const b2_lp_view& S, const double* Dr, c
         res->fp32_accepted = fin.fp32_accepted;
         res->final_eta = fin.eta;
         res->final_omega = fin.omega;
+        res->group_ctas = 1;
         res->objective = L.obj_offset;
         if (x_out)
             for (int32_t j = 0; j < L.n; ++j) res->objective += L.c[L.inv_c[j]] * x_out[j];

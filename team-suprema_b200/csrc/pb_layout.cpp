@@ -8,24 +8,25 @@
 // entries of y it finishes), and the destination chunk is cut into bins whose
 // entries fit the CTA's shared memory.
 //   * phase 1 (producer, the pass that computes v): CTA k multiplies each entry
-//     of its source chunk by v (held in its shared memory) and writes the
-//     products out in runs, one run per destination bin; each run is a
-//     contiguous piece of the product buffer.
+//     of its source chunk by v (held in its shared memory) and writes each
+//     product to its place in the product buffer; the chunk's entries are
+//     stored in the order of those places, so consecutive threads write
+//     consecutive places except where a destination bin ends.
 //   * phase 2 (consumer, the next pass): CTA k streams the products of each of
-//     its bins (all runs of the bin are adjacent), places each at its slot in
+//     its bins (a contiguous piece of the buffer), places each at its slot in
 //     shared memory, and sums every destination row's products in the order of
-//     the row's CSR entries (ascending source index), then runs the row's
-//     epilogue.
-// Every byte moves in long coalesced runs; the summation order is fixed by the
+//     the row's CSR entries (the order the entries were given in, as the
+//     reference's CSR builders fill rows), then runs the row's epilogue.
+// Every byte moves in coalesced streams; the summation order is fixed by the
 // layout, so the result is the same bits on every run.
 //
 // Layout (all in the engine's device order of rows and columns):
 //   product buffer : ordered by (bin t, source chunk p, CSR position q)
 //   slot[pos]      : q - first CSR position of the bin (uint16)
-//   producer list  : ordered by (source chunk p, bin t, q); loc = source index
-//                    within its chunk (uint16), val = the entry's value (FP32)
-//   run_start[p][t]: offset of run (p, t) in the producer list (T + 1 per p)
-//   run_dest[p][t] : offset of run (p, t) in the product buffer
+//   producer list  : ordered by (source chunk p, bin t, q); src_first[p] its
+//                    start; loc = source index within the chunk (uint16),
+//                    val = the entry's value (FP32), dest = its place in the
+//                    product buffer (int32)
 //   dst_ptr        : CSR offsets of the destination rows
 #include <algorithm>
 #include <cstdint>
@@ -35,11 +36,7 @@
 
 namespace b2 {
 
-namespace {
-
-// Splits [0, len) into `parts` contiguous chunks of about equal weight
-// (weight of index i: w[i] + 1), with no chunk above max_len indices.
-std::vector<int32_t> balanced_split(const std::vector<int32_t>& w, int32_t parts, int32_t max_len) {
+std::vector<int32_t> pb_split(const std::vector<int32_t>& w, int32_t parts, int32_t max_len) {
     const int32_t len = (int32_t)w.size();
     int64_t total = 0;
     for (int32_t v : w) total += v + 1;
@@ -55,34 +52,32 @@ std::vector<int32_t> balanced_split(const std::vector<int32_t>& w, int32_t parts
     return b;
 }
 
-}  // namespace
-
 bool build_pb(int32_t n_dst, int32_t n_src, const std::vector<int32_t>& dst, const std::vector<int32_t>& src,
-              const std::vector<float>& val, int32_t n_chunks, int32_t bin_entries, PbHost& P) {
+              const std::vector<float>& val, const std::vector<int32_t>& src_start,
+              const std::vector<int32_t>& dst_start, int32_t bin_entries, PbHost& P) {
     const int64_t nnz = (int64_t)dst.size();
-    if (n_chunks < 1 || nnz == 0 || nnz >= (int64_t)INT32_MAX || bin_entries > 65535) return false;
+    const int32_t n_chunks = (int32_t)src_start.size() - 1;
+    if (n_chunks < 1 || (int32_t)dst_start.size() != n_chunks + 1 || nnz == 0 || nnz >= (int64_t)INT32_MAX ||
+        bin_entries > 65535)
+        return false;
     P = PbHost();
     P.n_chunks = n_chunks;
-    // destination CSR, entries in ascending source order inside a row
-    std::vector<int32_t> dcnt(n_dst, 0), scnt(n_src, 0);
-    for (int64_t e = 0; e < nnz; ++e) { dcnt[dst[e]]++; scnt[src[e]]++; }
+    // destination CSR offsets
+    std::vector<int32_t> dcnt(n_dst, 0);
+    for (int64_t e = 0; e < nnz; ++e) dcnt[dst[e]]++;
     for (int32_t i = 0; i < n_dst; ++i)
         if (dcnt[i] > bin_entries) return false;  // a row must fit one bin
     P.dst_ptr.assign(n_dst + 1, 0);
     for (int32_t i = 0; i < n_dst; ++i) P.dst_ptr[i + 1] = P.dst_ptr[i] + dcnt[i];
     std::vector<int32_t> q_of(nnz);  // CSR position of entry e
     {
-        // counting sort by source, then stable by destination: rows in ascending source order
-        std::vector<int32_t> sp(n_src + 1, 0);
-        for (int32_t j = 0; j < n_src; ++j) sp[j + 1] = sp[j] + scnt[j];
-        std::vector<int32_t> by_src(nnz);
-        for (int64_t e = 0; e < nnz; ++e) by_src[sp[src[e]]++] = (int32_t)e;
+        // stable in the order the entries are given, as the reference's
+        // to_csr / to_csc_as_transposed_csr fill (include/sparse.hpp:24-50)
         std::vector<int32_t> cur(P.dst_ptr.begin(), P.dst_ptr.end() - 1);
-        for (int32_t e : by_src) q_of[e] = cur[dst[e]]++;
+        for (int64_t e = 0; e < nnz; ++e) q_of[e] = cur[dst[e]]++;
     }
-    // chunks: source and destination cut by entries, at most 65535 indices each
-    P.src_start = balanced_split(scnt, n_chunks, 65535);
-    P.dst_start = balanced_split(dcnt, n_chunks, 1 << 30);
+    P.src_start = src_start;
+    P.dst_start = dst_start;
     // bins inside each destination chunk
     P.dst_bin.assign(n_chunks + 1, 0);
     for (int32_t k = 0; k < n_chunks; ++k) {
@@ -115,48 +110,70 @@ bool build_pb(int32_t n_dst, int32_t n_src, const std::vector<int32_t>& dst, con
     for (int64_t e = 0; e < nnz; ++e) e_at[q_of[e]] = (int32_t)e;
     // run sizes (p, t)
     const size_t runs = (size_t)n_chunks * T;
-    std::vector<int32_t> cnt(runs, 0);
+    std::vector<int64_t> cnt(runs, 0);
     for (int32_t q = 0; q < (int32_t)nnz; ++q) {
         const int32_t e = e_at[q];
         cnt[(size_t)chunk_of[src[e]] * T + bin_of[dst[e]]]++;
     }
-    // product buffer: by (t, p, q); run_dest[p][t]
-    P.run_dest.assign(runs, 0);
+    // product buffer by (t, p, q): place of run (p, t); producer list by (p, t, q): start of run (p, t)
+    std::vector<int64_t> run_place(runs, 0), run_first(runs, 0);
     {
         int64_t off = 0;
         for (int32_t t = 0; t < T; ++t)
             for (int32_t p = 0; p < n_chunks; ++p) {
-                P.run_dest[(size_t)p * T + t] = (int32_t)off;
+                run_place[(size_t)p * T + t] = off;
                 off += cnt[(size_t)p * T + t];
             }
-    }
-    // producer list: by (p, t, q); run_start[p][t]
-    P.run_start.assign((size_t)n_chunks * (T + 1), 0);
-    {
-        int64_t off = 0;
+        off = 0;
+        P.src_first.assign(n_chunks + 1, 0);
         for (int32_t p = 0; p < n_chunks; ++p) {
+            P.src_first[p] = (int32_t)off;
             for (int32_t t = 0; t < T; ++t) {
-                P.run_start[(size_t)p * (T + 1) + t] = (int32_t)off;
+                run_first[(size_t)p * T + t] = off;
                 off += cnt[(size_t)p * T + t];
             }
-            P.run_start[(size_t)p * (T + 1) + T] = (int32_t)off;
         }
+        P.src_first[n_chunks] = (int32_t)off;
     }
     P.loc.resize(nnz);
     P.val.resize(nnz);
+    P.dest.resize(nnz);
     P.slot.resize(nnz);
-    std::vector<int32_t> fill(runs, 0);
+    std::vector<int64_t> fill(runs, 0);
     for (int32_t q = 0; q < (int32_t)nnz; ++q) {  // CSR order: q ascending inside every run
         const int32_t e = e_at[q];
         const int32_t p = chunk_of[src[e]], t = bin_of[dst[e]];
         const size_t r = (size_t)p * T + t;
-        const int32_t k = fill[r]++;
-        const int32_t at = P.run_start[(size_t)p * (T + 1) + t] + k;
+        const int64_t k = fill[r]++;
+        const int64_t at = run_first[r] + k, place = run_place[r] + k;
         P.loc[at] = (uint16_t)(src[e] - P.src_start[p]);
         P.val[at] = val[e];
-        P.slot[P.run_dest[r] + k] = (uint16_t)(q - P.dst_ptr[P.bin_first[t]]);
+        P.dest[at] = (int32_t)place;
+        P.slot[place] = (uint16_t)(q - P.dst_ptr[P.bin_first[t]]);
     }
     return true;
+}
+
+// y = M x through the two-phase layout on the host, phase by phase as the
+// device runs it (products placed by dest, bins summed from their slots in
+// CSR order): the check of the layout that needs no GPU.
+void pb_spmv_host(const PbHost& P, int32_t n_dst, const double* x, double* y) {
+    std::vector<double> prod(P.dest.size());
+    for (int32_t k = 0; k < P.n_chunks; ++k)
+        for (int32_t i = P.src_first[k]; i < P.src_first[k + 1]; ++i)
+            prod[P.dest[i]] = (double)P.val[i] * x[P.src_start[k] + P.loc[i]];
+    std::vector<double> bin((size_t)std::max(P.max_bin_entries, 1));
+    for (int32_t t = 0; t < P.n_bins; ++t) {
+        const int32_t r0 = P.bin_first[t], r1 = P.bin_first[t + 1];
+        const int32_t s = P.dst_ptr[r0], e = P.dst_ptr[r1];
+        for (int32_t q = s; q < e; ++q) bin[P.slot[q]] = prod[q];
+        for (int32_t i = r0; i < r1; ++i) {
+            double acc = 0.0;
+            for (int32_t z = P.dst_ptr[i] - s; z < P.dst_ptr[i + 1] - s; ++z) acc += bin[z];
+            y[i] = acc;
+        }
+    }
+    (void)n_dst;
 }
 
 }  // namespace b2

@@ -868,6 +868,7 @@ struct ServerImpl {
                 p += 8 * (size_t)r->meta.n;
                 r->y.assign(reinterpret_cast<const double*>(p), reinterpret_cast<const double*>(p) + r->meta.m);
                 fill_result(f, r->res);
+                r->res.group_ctas = r->cluster && max_clusters > 0 ? dev::kMaxCluster : 1;
                 r->res.device_ms = (double)(t1 - t0) * 1e-6;
                 set_objective(r);
             }
