@@ -86,17 +86,7 @@ typedef struct b2_solve_opts {
        a set stop_flag does. NULL: not used. */
     int32_t (*stop_poll)(void* stop_ctx);
     void* stop_ctx;
-    int32_t product;          /* whole-GPU engine, A x and A^T y: B2_PRODUCT_* (read at create and solve) */
 } b2_solve_opts;
-
-/* B2_PRODUCT_AUTO: two-phase products for large LPs with short rows and
- * columns (random sparsity: every gather would be its own memory sector),
- * sliced-ELL gathers otherwise. TWO_PHASE: two-phase wherever the matrix fits
- * the format. SLICED: gathers only. Both are deterministic; they add a row's
- * entries in different orders, so their last bits differ. */
-#define B2_PRODUCT_AUTO 0
-#define B2_PRODUCT_SLICED 1
-#define B2_PRODUCT_TWO_PHASE 2
 
 void b2_default_opts(b2_solve_opts* opts);
 
@@ -191,7 +181,6 @@ typedef struct b2_engine_info {
     int32_t ctas, threads_per_cta; /* persistent-kernel launch shape */
     int32_t sm_count;
     int64_t device_bytes;          /* HBM held by the engine */
-    int32_t two_phase;             /* 1: A x' and A^T y' run as two-phase products (a full-size launch) */
 } b2_engine_info;
 int b2_engine_get_info(b2_engine* e, b2_engine_info* info);
 
@@ -386,14 +375,6 @@ int b2_scale(const b2_lp_view* lp, int32_t ruiz_passes, double* val_s, double* c
  * does. For ingest of large LPs, whose host scaling takes seconds. */
 int b2_scale_gpu(const b2_lp_view* lp, int32_t ruiz_passes, double* val_s, double* c_s, double* rL_s,
                  double* rU_s, double* l_s, double* u_s, double* Dr, double* Dc);
-
-/* y = A x (A's values rounded to FP32, x and y FP64, entries added in CSR
- * order) through the two-phase product layout the whole-GPU engine uses
- * (team-suprema_b200/csrc/pb_layout.cpp), evaluated on the host phase by
- * phase: `chunks` source / destination chunks, bins of at most `bin_entries`
- * products. No counterpart in the reference; it checks the layout without a
- * GPU. B2_ERR_UNSUPPORTED when the matrix does not fit the format. */
-int b2_two_phase_spmv_host(const b2_lp_view* lp, int32_t chunks, int32_t bin_entries, const double* x, double* y);
 
 /* PDLP form of a ranged LP, as build_pdlp_form (src/pdlp.cpp:8-82) builds it:
  * equality rows first in input order, then the one-sided rows in input order

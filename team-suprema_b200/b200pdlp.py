@@ -34,7 +34,6 @@ INCLUDE_H = os.path.join(os.path.dirname(HERE), "include", "b200_pdlp.h")
 B2_OK, B2_ERR_INVALID, B2_ERR_CUDA, B2_ERR_OOM, B2_ERR_TIMEOUT, B2_ERR_NO_DEVICE, B2_ERR_NONFINITE, \
     B2_ERR_UNSUPPORTED, B2_ERR_PENDING, B2_ERR_INFEASIBLE, B2_ERR_UNBOUNDED = range(11)
 PREC_FP64, PREC_MIXED = 0, 1
-PRODUCT_AUTO, PRODUCT_SLICED, PRODUCT_TWO_PHASE = 0, 1, 2
 EXIT_CONVERGED, EXIT_MAX_ITER, EXIT_STOPPED, EXIT_TIME_LIMIT = 1, 2, 3, 4
 
 EXPORTED = [
@@ -45,7 +44,7 @@ EXPORTED = [
     "b2_batch_destroy",
     "b2_server_create", "b2_server_submit", "b2_server_submit_file", "b2_server_submit_lp", "b2_server_wait",
     "b2_server_stats_get", "b2_pdlp_form_build", "b2_pdlp_form_view", "b2_pdlp_form_extract",
-    "b2_pdlp_form_destroy", "b2_two_phase_spmv_host", "b2_presolve", "b2_presolved_view", "b2_postsolve", "b2_presolved_destroy",
+    "b2_pdlp_form_destroy", "b2_presolve", "b2_presolved_view", "b2_postsolve", "b2_presolved_destroy",
     "b2_server_destroy", "b2_lp_write", "b2_lp_read_dims", "b2_lp_read",
     "b2_layout_digest", "b2_request_work", "b2_shard_plan", "b2_pool_create", "b2_pool_submit", "b2_pool_submit_file",
     "b2_pool_wait", "b2_pool_stats_get", "b2_pool_destroy",
@@ -75,8 +74,7 @@ class SolveOpts(C.Structure):
                 ("time_limit_s", C.c_double), ("barrier_timeout_s", C.c_double), ("max_ctas", C.c_int32),
                 ("lane_target", C.c_int32), ("sigma_window", C.c_int32), ("return_current", C.c_int32),
                 ("stream", C.c_void_p), ("debug_delay_us", C.c_int32), ("batch_cluster_nnz", C.c_int32),
-                ("batch_block", C.c_int32), ("stop_poll", C.c_void_p), ("stop_ctx", C.c_void_p),
-                ("product", C.c_int32)]
+                ("batch_block", C.c_int32), ("stop_poll", C.c_void_p), ("stop_ctx", C.c_void_p)]
 
 
 class _Result(C.Structure):
@@ -117,7 +115,7 @@ class EngineInfo(C.Structure):
     _fields_ = [("m", C.c_int32), ("n", C.c_int32), ("nnz", C.c_int64), ("a_slices", C.c_int64),
                 ("at_slices", C.c_int64), ("a_padded", C.c_int64), ("at_padded", C.c_int64),
                 ("values_exact_fp32", C.c_int32), ("ctas", C.c_int32), ("threads_per_cta", C.c_int32),
-                ("sm_count", C.c_int32), ("device_bytes", C.c_int64), ("two_phase", C.c_int32)]
+                ("sm_count", C.c_int32), ("device_bytes", C.c_int64)]
 
 
 _lib = None
@@ -164,7 +162,6 @@ def lib():
             L.b2_server_submit_file.argtypes = [vp, C.c_char_p, C.POINTER(i64)]
             L.b2_server_submit_lp.argtypes = [vp, C.POINTER(_LPView), i32, C.POINTER(i64)]
             L.b2_pdlp_form_build.argtypes = [C.POINTER(_LPView), C.POINTER(vp)]
-            L.b2_two_phase_spmv_host.argtypes = [C.POINTER(_LPView), i32, i32, vp, vp]
             L.b2_pdlp_form_view.argtypes = [vp, C.POINTER(_LPView)]
             L.b2_pdlp_form_view.restype = None
             L.b2_pdlp_form_extract.argtypes = [vp, vp, vp, vp, vp]
@@ -857,16 +854,6 @@ class Presolved:
         if getattr(self, "_h", None) and self._h.value:
             lib().b2_presolved_destroy(self._h)
             self._h = C.c_void_p()
-
-
-def two_phase_spmv_host(lp: RangedLP, x, chunks: int = 296, bin_entries: int = 8192) -> np.ndarray:
-    """y = A x through the engine's two-phase product layout, evaluated on the
-    host (b2_two_phase_spmv_host): the layout's check without a GPU."""
-    L = RangedLP.like(lp)
-    xx = _vec(x, L.n)
-    y = np.zeros(max(L.m, 1))
-    _check(lib().b2_two_phase_spmv_host(C.byref(L.view()), int(chunks), int(bin_entries), _ptr(xx), _ptr(y)))
-    return y[:L.m]
 
 
 def version() -> str:

@@ -208,25 +208,6 @@ int b2_server_submit_lp(b2_server* s, const b2_lp_view* original, int32_t presol
     });
 }
 
-int b2_two_phase_spmv_host(const b2_lp_view* lp, int32_t chunks, int32_t bin_entries, const double* x, double* y) {
-    return b2::guarded([&] {
-        if (!lp || !x || !y || chunks < 1) b2::fail(B2_ERR_INVALID, "bad argument");
-        std::vector<int32_t> rows(lp->row_idx, lp->row_idx + lp->nnz), cols(lp->col_idx, lp->col_idx + lp->nnz);
-        std::vector<float> vals(lp->nnz);
-        std::vector<int32_t> rc(lp->m, 0), cc(lp->n, 0);
-        for (int64_t e = 0; e < lp->nnz; ++e) {
-            vals[e] = (float)lp->val[e];
-            rc[rows[e]]++;
-            cc[cols[e]]++;
-        }
-        b2::PbHost P;
-        if (!b2::build_pb(lp->m, lp->n, rows, cols, vals, b2::pb_split(cc, chunks, 65535), b2::pb_split(rc, chunks, 65535),
-                          bin_entries, P))
-            b2::fail(B2_ERR_UNSUPPORTED, "the matrix does not fit the two-phase format");
-        b2::pb_spmv_host(P, lp->m, x, y);
-    });
-}
-
 int b2_pdlp_form_build(const b2_lp_view* ranged, b2_pdlp_form** out) {
     return b2::guarded([&] {
         if (!ranged || !out) b2::fail(B2_ERR_INVALID, "null argument");

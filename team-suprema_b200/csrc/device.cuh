@@ -83,23 +83,6 @@ struct SellDev {
     unsigned* seg_cnt;
 };
 
-// Two-phase product y = M v (pb_layout.cpp): the device copy of PbHost plus
-// the product buffer (nnz elements of the iterate type).
-struct PbDev {
-    int n_chunks, n_bins;
-    const int* src_start;
-    const int* dst_start;
-    const int* dst_bin;
-    const int* bin_first;
-    const int* dst_ptr;
-    const int* src_first;
-    const uint16_t* loc;
-    const float* val;
-    const int* dest;
-    const uint16_t* slot;
-    void* prod;
-};
-
 template <class T>
 struct Bufs {
     T* x[2];
@@ -147,12 +130,6 @@ struct KParamsBase {
     unsigned long long debug_delay_ns;  // test hook: the group's first CTA arrives late at its first barrier
     double* trace;                      // per-check records (kTraceFields doubles), may be null
     int trace_cap;
-    // two-phase products (whole-GPU launch whose CTA count equals pbA.n_chunks):
-    // A x' from pbA (columns -> rows), A^T y' from pbAT (rows -> columns); the
-    // CTA's dynamic shared memory holds a bin of products (pb_bin entries)
-    // and its chunk of the vector it produces
-    int pb, pb_bin;
-    PbDev pbA, pbAT;
 };
 
 template <class T>
@@ -194,8 +171,6 @@ struct Group {
     // for A^T y'), used when both fit; null: gathers read global memory
     unsigned char* svec = nullptr;
     int svec_bytes = 0;
-    // GK_GRID with two-phase products: the CTA's dynamic shared memory
-    unsigned char* pbs = nullptr;
 };
 
 // ------------------------------------------------------------- primitives
@@ -212,13 +187,6 @@ __device__ __forceinline__ uint32_t ld_mat(const uint32_t* p) {
     uint32_t v;
     if (KEEP) asm("ld.global.nc.u32 %0, [%1];" : "=r"(v) : "l"(p));
     else asm("ld.global.nc.L1::no_allocate.u32 %0, [%1];" : "=r"(v) : "l"(p));
-    return v;
-}
-template <bool KEEP>
-__device__ __forceinline__ uint16_t ld_mat(const uint16_t* p) {
-    unsigned short v;
-    if (KEEP) asm("ld.global.nc.u16 %0, [%1];" : "=h"(v) : "l"(p));
-    else asm("ld.global.nc.L1::no_allocate.u16 %0, [%1];" : "=h"(v) : "l"(p));
     return v;
 }
 template <bool KEEP>
@@ -702,154 +670,6 @@ __device__ void pass_cols_step(const KParams<T>& P, const Ctl& c, const Group& g
     }
 }
 
-// ---------------------------------------------- two-phase products (GK_GRID)
-//
-// Phase 1: this CTA's products of its source chunk k, from the chunk's values
-// sv in shared memory: prod[dest[i]] = val[i] * sv[loc[i]] over the chunk's
-// producer entries (coalesced streams in, runs out). Phase 2 (pb_consume):
-// the products of each destination bin of chunk k land in shared memory at
-// their slots, then every destination row adds its products in CSR order and
-// runs the pass's epilogue on the sum. Between the phases lies a grid barrier.
-template <class T>
-__device__ __forceinline__ void pb_produce(const PbDev& D, int k, const T* sv) {
-    const int b = __ldg(D.src_first + k), e = __ldg(D.src_first + k + 1);
-    T* prod = static_cast<T*>(D.prod);
-    const uint32_t* dest = reinterpret_cast<const uint32_t*>(D.dest);
-    const int nt = blockDim.x;
-    int i = b + (int)threadIdx.x;
-    for (; i + 3 * nt < e; i += 4 * nt) {
-        uint16_t lc[4];
-        float vv[4];
-        uint32_t dd[4];
-#pragma unroll
-        for (int u = 0; u < 4; ++u) {
-            lc[u] = ld_mat<false>(D.loc + i + u * nt);
-            vv[u] = ld_mat<false>(D.val + i + u * nt);
-            dd[u] = ld_mat<false>(dest + i + u * nt);
-        }
-#pragma unroll
-        for (int u = 0; u < 4; ++u) prod[dd[u]] = (T)vv[u] * sv[lc[u]];
-    }
-    for (; i < e; i += nt) prod[ld_mat<false>(dest + i)] = (T)ld_mat<false>(D.val + i) * sv[ld_mat<false>(D.loc + i)];
-}
-
-template <class T, class Epi>
-__device__ __forceinline__ void pb_consume(const PbDev& D, int k, T* sbuf, Epi&& epi) {
-    const int t0 = __ldg(D.dst_bin + k), t1 = __ldg(D.dst_bin + k + 1);
-    const T* prod = static_cast<const T*>(D.prod);
-    const int nt = blockDim.x;
-    for (int t = t0; t < t1; ++t) {
-        const int r0 = __ldg(D.bin_first + t), r1 = __ldg(D.bin_first + t + 1);
-        const int s = __ldg(D.dst_ptr + r0), e = __ldg(D.dst_ptr + r1);
-        int q = s + (int)threadIdx.x;
-        for (; q + 3 * nt < e; q += 4 * nt) {
-            uint16_t sl[4];
-            T pv[4];
-#pragma unroll
-            for (int u = 0; u < 4; ++u) {
-                sl[u] = ld_mat<false>(D.slot + q + u * nt);
-                pv[u] = __ldcg(prod + q + u * nt);
-            }
-#pragma unroll
-            for (int u = 0; u < 4; ++u) sbuf[sl[u]] = pv[u];
-        }
-        for (; q < e; q += nt) sbuf[ld_mat<false>(D.slot + q)] = __ldcg(prod + q);
-        __syncthreads();
-        for (int i = r0 + (int)threadIdx.x; i < r1; i += nt) {
-            const int a = __ldg(D.dst_ptr + i) - s, b = __ldg(D.dst_ptr + i + 1) - s;
-            T acc = T(0);
-            for (int z = a; z < b; ++z) acc += sbuf[z];
-            epi(i, acc);
-        }
-        __syncthreads();
-    }
-}
-
-// Rows pass, two-phase: (A x')_i from the products the columns pass wrote,
-// the dual step and its statistics exactly as pass_rows_step, y' of the
-// CTA's row chunk kept in shared memory; then the A^T products of y'.
-template <class T>
-__device__ void pass_rows_step_pb(const KParams<T>& P, const Ctl& c, const Group& g, double* v, T* sbuf, T* svec) {
-    const T* y = P.it.y[c.yi];
-    T* yn = P.it.y[1 - c.yi];
-    const T* ax = P.it.ax[c.ax_cur];
-    T* axn = P.it.ax[c.ax_nxt];
-    const double sigma = c.eta * c.omega, pend = c.pend_y;
-    const int k = g.rank;
-    const int r0 = __ldg(P.pbA.dst_start + k);
-    pb_consume<T>(P.pbA, k, sbuf, [&](int row, T acc) {
-        const T yv = ld_it<GK_GRID>(y + row), axv = ld_it<GK_GRID>(ax + row);
-        const double w = __ldg(P.dr2 + row), brow = __ldg(P.b + row);
-        const double aw = fabs(w);
-        double nv = (double)yv + sigma * aw * (brow - (2.0 * (double)acc - (double)axv));
-        if (w < 0.0 && nv < 0.0) nv = 0.0;
-        const T nt = (T)nv;
-        yn[row] = nt;
-        svec[row - r0] = nt;
-        axn[row] = acc;
-        const double d = (double)nt - (double)yv;
-        v[0] += d * d / aw;
-        v[1] += d * ((double)acc - (double)axv);
-        if (pend != 0.0) P.ysum[row] += pend * (double)yv;
-    });
-    __syncthreads();  // y' of the whole chunk is in svec (also when the chunk has no bin)
-    pb_produce<T>(P.pbAT, k, svec);
-}
-
-// Primal step of column j (as primal_col) that also keeps x'_j in the CTA's chunk vector.
-template <class T>
-__device__ __forceinline__ void primal_col_pb(const KParams<T>& P, int j, T xv, double gj, double tau, T* xn,
-                                              double& dx2, T* svj) {
-    double lj, uj;
-    col_bounds(P, j, lj, uj);
-    const double w = __ldg(P.dc2 + j);
-    double v = (double)xv - tau * w * (__ldg(P.c + j) - gj);
-    v = fmin(fmax(v, lj), uj);
-    const T vt = (T)v;
-    xn[j] = vt;
-    *svj = vt;
-    const double d = (double)vt - (double)xv;
-    dx2 += d * d / w;
-}
-
-// Columns pass, two-phase: [accepted] (A^T y')_j from the rows pass's
-// products and the x-average update, then the primal step of the next attempt
-// on the CTA's column chunk; then the A products of x'.
-template <class T>
-__device__ void pass_cols_step_pb(const KParams<T>& P, const Ctl& c, const Group& g, double& dx2, T* sbuf, T* svec) {
-    const T* x = P.it.x[c.xi];
-    T* xn = P.it.x[1 - c.xi];
-    T* aty = P.it.aty[c.aty_cur];
-    const double tau = c.eta / c.omega, pend = c.pend_x;
-    const int k = g.rank;
-    const int c0 = __ldg(P.pbAT.dst_start + k), c1 = __ldg(P.pbAT.dst_start + k + 1);
-    if (c.last_accepted) {
-        pb_consume<T>(P.pbAT, k, sbuf, [&](int j, T acc) {
-            const T xv = ld_it<GK_GRID>(x + j);
-            aty[j] = acc;
-            if (pend != 0.0) P.xsum[j] += pend * (double)xv;
-            primal_col_pb<T>(P, j, xv, (double)acc, tau, xn, dx2, svec + (j - c0));
-        });
-    } else {
-        for (int j = c0 + (int)threadIdx.x; j < c1; j += (int)blockDim.x)
-            primal_col_pb<T>(P, j, ld_it<GK_GRID>(x + j), (double)ld_it<GK_GRID>(aty + j), tau, xn, dx2,
-                             svec + (j - c0));
-    }
-    __syncthreads();  // x' of the whole chunk is in svec
-    pb_produce<T>(P.pbA, k, svec);
-}
-
-// The A products of x' (already in global memory) for the CTA's column chunk:
-// after a restart, or a resume from a yield.
-template <class T>
-__device__ void pb_produce_from(const KParams<T>& P, const Group& g, const T* xg, T* svec) {
-    const int k = g.rank;
-    const int c0 = __ldg(P.pbA.src_start + k), c1 = __ldg(P.pbA.src_start + k + 1);
-    for (int j = c0 + (int)threadIdx.x; j < c1; j += (int)blockDim.x) svec[j - c0] = __ldcg(xg + j);
-    __syncthreads();
-    pb_produce<T>(P.pbA, k, svec);
-}
-
 // KKT check, rows (verify.cpp:35-87 row terms) for the current and average
 // points, the average's A x, the restart distance of y, and the pending
 // y-average update.
@@ -1144,11 +964,6 @@ __device__ bool solve_body(const KParams<T>& P, const Group& g) {
         sx = reinterpret_cast<T*>(g.svec);
         sy = sx + P.n;
     }
-    // whole-GPU launch with two-phase products: a bin of products and the
-    // CTA's chunk of the vector it produces, in dynamic shared memory
-    const bool pbon = GK == GK_GRID && P.pb && g.pbs;
-    T* pb_sbuf = pbon ? reinterpret_cast<T*>(g.pbs) : nullptr;
-    T* pb_svec = pbon ? pb_sbuf + P.pb_bin : nullptr;
 
     // ---------------------------------------------------------- start-up
     if (s.mode == MODE_CONTINUE) {
@@ -1166,10 +981,6 @@ __device__ bool solve_body(const KParams<T>& P, const Group& g) {
         if (sx)
             for (int j = g.gt; j < P.n; j += g.nt) sx[j] = ld_it<GK>(P.it.x[1 - s.xi] + j);
         __syncthreads();
-        if (pbon) {  // the A products of x' left by the yield
-            pb_produce_from<T>(P, g, P.it.x[1 - s.xi], pb_svec);
-            if (!group_sync<GK>(g)) return false;
-        }
     } else {
         if (s.mode == MODE_START) {
             // x = x0, y = 0, A^T y = 0, sums = 0 (pdlp_algo.hpp:68-84)
@@ -1230,18 +1041,9 @@ __device__ bool solve_body(const KParams<T>& P, const Group& g) {
         {   // primal step of the first attempt
             double dx2[1] = {0.0};
             const double tau = s.eta / s.omega;
-            if (pbon) {
-                const int c0 = __ldg(P.pbA.src_start + g.rank), c1 = __ldg(P.pbA.src_start + g.rank + 1);
-                for (int j = c0 + tid; j < c1; j += (int)blockDim.x)
-                    primal_col_pb<T>(P, j, ld_it<GK>(P.it.x[s.xi] + j), (double)ld_it<GK>(P.it.aty[s.aty_cur] + j),
-                                     tau, P.it.x[1 - s.xi], dx2[0], pb_svec + (j - c0));
-                __syncthreads();
-                pb_produce<T>(P.pbA, g.rank, pb_svec);
-            } else {
-                for (int j = g.gt; j < P.n; j += g.nt)
-                    primal_col<T>(P, j, ld_it<GK>(P.it.x[s.xi] + j), (double)ld_it<GK>(P.it.aty[s.aty_cur] + j), tau,
-                                  P.it.x[1 - s.xi], dx2[0], sx);
-            }
+            for (int j = g.gt; j < P.n; j += g.nt)
+                primal_col<T>(P, j, ld_it<GK>(P.it.x[s.xi] + j), (double)ld_it<GK>(P.it.aty[s.aty_cur] + j), tau,
+                              P.it.x[1 - s.xi], dx2[0], sx);
             cta_partial<1, GK>(dx2, g, SLOT_X, s_red);
         }
         if (!group_sync<GK>(g)) return false;
@@ -1265,8 +1067,7 @@ __device__ bool solve_body(const KParams<T>& P, const Group& g) {
             if (poll && g.rank == 0 && tid == 0 && P.host_stop) hstop = *P.host_stop;
             {
                 double v[2] = {0.0, 0.0};
-                if (pbon) pass_rows_step_pb<T>(P, s, g, v, pb_sbuf, pb_svec);
-                else pass_rows_step<GK, T, V>(P, s, g, lane, v, sx, sy);
+                pass_rows_step<GK, T, V>(P, s, g, lane, v, sx, sy);
                 cta_partial<2, GK>(v, g, SLOT_A, s_red);
             }
             if (g.rank == 0 && tid == 0) {
@@ -1316,8 +1117,7 @@ __device__ bool solve_body(const KParams<T>& P, const Group& g) {
             // ---- cols pass: A^T y' (if accepted) + next primal step ----
             {
                 double dx2[1] = {0.0};
-                if (pbon) pass_cols_step_pb<T>(P, s, g, dx2[0], pb_sbuf, pb_svec);
-                else pass_cols_step<GK, T, V>(P, s, g, lane, dx2[0], sx, sy);
+                pass_cols_step<GK, T, V>(P, s, g, lane, dx2[0], sx, sy);
                 cta_partial<1, GK>(dx2, g, SLOT_X, s_red);
             }
             if (tid == 0) {
@@ -1348,10 +1148,6 @@ __device__ bool solve_body(const KParams<T>& P, const Group& g) {
                     t = s.aty_cur; s.aty_cur = s.aty_avg; s.aty_avg = t;
                 }
                 if (!group_sync<GK>(g)) return false;
-                if (pbon && restart) {  // the restart moved x': its A products again
-                    pb_produce_from<T>(P, g, P.it.x[1 - s.xi], pb_svec);
-                    if (!group_sync<GK>(g)) return false;
-                }
             }
         }
         if (s.switch_req || s.exit_reason != 0) break;

@@ -29,12 +29,10 @@ struct GridArgs {
     unsigned long long timeout_ns;
     unsigned long long yield_ns;  // the solve yields this long after the launch starts; 0: never
     int svec_bytes;               // one-CTA launch: dynamic shared memory for staged x' / y'
-    int pb_smem;                  // whole-GPU launch with two-phase products: its dynamic shared memory
 };
 
 template <class T, class V>
 __global__ void __launch_bounds__(kBlock, 2) k_pdlp(const KParams<T> P, const GridArgs ga) {
-    extern __shared__ __align__(16) unsigned char s_pb[];
     Group g;
     g.rank = blockIdx.x;
     g.size = gridDim.x;
@@ -49,7 +47,6 @@ __global__ void __launch_bounds__(kBlock, 2) k_pdlp(const KParams<T> P, const Gr
     g.timeout_ns = ga.timeout_ns;
     g.spart = nullptr;
     if (ga.yield_ns) g.yield_at = gtimer() + ga.yield_ns;  // read on CTA 0 only
-    g.pbs = ga.pb_smem > 0 ? s_pb : nullptr;
     solve_body<GK_GRID, T, V>(P, g);
 }
 
@@ -134,15 +131,6 @@ struct EngineImpl {
     int* d_stop = nullptr;
     int max_ctas = 0;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
-    // two-phase products (pb_layout.cpp): ready when built; used by a launch of pb_chunks CTAs
-    static constexpr int kPbBin = 8192;        // products of one destination bin (shared memory)
-    static constexpr int kPbChunkCap = 4096;   // indices of one source chunk (shared memory)
-    static constexpr int64_t kPbMinNnz = 1 << 20;
-    bool pb_ready = false;
-    bool use_two_phase = true;  // the solve's b2_solve_opts::product allows it
-    int pb_chunks = 0;
-    size_t pb_smem32 = 0, pb_smem64 = 0;
-    dev::PbDev pbA{}, pbAT{};
 
     cudaMemPool_t mpool = nullptr;
 
@@ -222,77 +210,6 @@ struct EngineImpl {
         bp.threads = (int)std::max(1u, std::min(8u, std::thread::hardware_concurrency()));
         build_layout(U, S, Dr, Dc, bp, L);
         create_device();
-        if (o.product != B2_PRODUCT_SLICED) build_two_phase(U, o);
-    }
-
-    dev::PbDev upload_pb(const PbHost& H) {
-        dev::PbDev d{};
-        d.n_chunks = H.n_chunks;
-        d.n_bins = H.n_bins;
-        d.src_start = up(H.src_start);
-        d.dst_start = up(H.dst_start);
-        d.dst_bin = up(H.dst_bin);
-        d.bin_first = up(H.bin_first);
-        d.dst_ptr = up(H.dst_ptr);
-        d.src_first = up(H.src_first);
-        d.loc = up(H.loc);
-        d.val = up(H.val);
-        d.dest = up(H.dest);
-        d.slot = up(H.slot);
-        d.prod = alloc<double>((size_t)L.nnz);
-        return d;
-    }
-
-    // Two-phase products for A x' and A^T y' (pb_layout.cpp). Automatic for
-    // large LPs whose rows and columns are short (every gather its own
-    // sector); one chunk of rows and of columns per co-resident CTA.
-    void build_two_phase(const b2_lp_view& U, const b2_solve_opts& o) {
-        const bool forced = o.product == B2_PRODUCT_TWO_PHASE;
-        if (!L.exact32 || L.nnz == 0) return;
-        if (!forced && L.nnz < kPbMinNnz) return;
-        std::vector<int32_t> rcnt(L.m, 0), ccnt(L.n, 0);
-        for (int64_t e = 0; e < U.nnz; ++e) { rcnt[L.inv_r[U.row_idx[e]]]++; ccnt[L.inv_c[U.col_idx[e]]]++; }
-        const int32_t rmax = L.m ? *std::max_element(rcnt.begin(), rcnt.end()) : 0;
-        const int32_t cmax = L.n ? *std::max_element(ccnt.begin(), ccnt.end()) : 0;
-        const int32_t lim = forced ? kPbBin : 256;  // each row is summed by one thread
-        if (rmax > lim || cmax > lim) return;
-        const size_t smem64 = sizeof(double) * (kPbBin + kPbChunkCap);
-        int per_sm = 1 << 30;
-        const void* ks[3] = {(const void*)dev::k_pdlp<float, float>, (const void*)dev::k_pdlp<double, float>,
-                             (const void*)dev::k_pdlp<double, double>};
-        for (const void* k : ks) {
-            cuda_ok(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem64), "attr");
-            int occ = 0;
-            cuda_ok(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k, dev::kBlock, smem64), "occ");
-            per_sm = std::min(per_sm, occ);
-        }
-        if (per_sm < 1) return;
-        // one chunk per CTA of the launch a solve with these options makes
-        const int chunks = pick_ctas(o);
-        if (chunks < 2 || chunks > per_sm * sm_count) return;
-        // the entries in device order
-        std::vector<int32_t> rows(U.nnz), cols(U.nnz);
-        std::vector<float> vals(U.nnz);
-        for (int64_t e = 0; e < U.nnz; ++e) {
-            rows[e] = L.inv_r[U.row_idx[e]];
-            cols[e] = L.inv_c[U.col_idx[e]];
-            vals[e] = (float)U.val[e];
-        }
-        const std::vector<int32_t> rsplit = pb_split(rcnt, chunks, kPbChunkCap);
-        const std::vector<int32_t> csplit = pb_split(ccnt, chunks, kPbChunkCap);
-        for (int k = 0; k < chunks; ++k)
-            if (rsplit[k + 1] - rsplit[k] > kPbChunkCap || csplit[k + 1] - csplit[k] > kPbChunkCap) return;
-        PbHost a, at;
-        if (!build_pb(L.m, L.n, rows, cols, vals, csplit, rsplit, kPbBin, a)) return;
-        if (!build_pb(L.n, L.m, cols, rows, vals, rsplit, csplit, kPbBin, at)) return;
-        const int chunk = std::max(a.max_src_chunk, at.max_src_chunk);
-        pb_smem64 = (sizeof(double) * (size_t)(kPbBin + chunk) + 15) / 16 * 16;
-        pb_smem32 = (sizeof(float) * (size_t)(kPbBin + chunk) + 15) / 16 * 16;
-        pbA = upload_pb(a);
-        pbAT = upload_pb(at);
-        pb_chunks = chunks;
-        pb_ready = true;
-        cuda_ok(cudaStreamSynchronize(stream), "two-phase upload");
     }
 
     void create_device() {
@@ -411,19 +328,8 @@ struct EngineImpl {
             cuda_ok(cudaGetLastError(), "k_pdlp_cta");
             return;
         }
-        dev::KParams<T> Q = P;
-        dev::GridArgs gq = ga;
-        size_t dyn = 0;
-        Q.pb = pb_ready && use_two_phase && ctas == pb_chunks ? 1 : 0;
-        if (Q.pb) {
-            Q.pb_bin = kPbBin;
-            Q.pbA = pbA;
-            Q.pbAT = pbAT;
-            dyn = sizeof(T) == 8 ? pb_smem64 : pb_smem32;
-        }
-        gq.pb_smem = (int)dyn;
-        void* args[] = {(void*)&Q, (void*)&gq};
-        cuda_ok(cudaLaunchCooperativeKernel((const void*)dev::k_pdlp<T, V>, dim3(ctas), dim3(dev::kBlock), args, dyn, st),
+        void* args[] = {(void*)&P, (void*)&ga};
+        cuda_ok(cudaLaunchCooperativeKernel((const void*)dev::k_pdlp<T, V>, dim3(ctas), dim3(dev::kBlock), args, 0, st),
                 "cudaLaunchCooperativeKernel");
     }
 
@@ -432,7 +338,6 @@ struct EngineImpl {
         auto t_host0 = std::chrono::steady_clock::now();
         cudaStream_t st = o.stream ? (cudaStream_t)o.stream : stream;
         if (o.max_iterations < 0) fail(B2_ERR_INVALID, "max_iterations < 0");
-        use_two_phase = o.product != B2_PRODUCT_SLICED;
         dev::Ctl h{};
         h.eta = L.eta0;
         h.omega = L.omega0;
@@ -702,7 +607,6 @@ void engine_info(EngineImpl* e, b2_engine_info* info) {
     info->threads_per_cta = dev::kBlock;
     info->sm_count = e->sm_count;
     info->device_bytes = (int64_t)e->bytes;
-    info->two_phase = e->pb_ready && info->ctas == e->pb_chunks ? 1 : 0;
 }
 
 void engine_spmv(EngineImpl* e, int which, const double* x, double* y) { e->spmv(which, x, y); }

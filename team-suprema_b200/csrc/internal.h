@@ -48,36 +48,6 @@ struct SellHost {
     int64_t n_groups() const { return (int64_t)seg.size() / 2; }
 };
 
-// Two-phase product y = M v of the whole-GPU engine (pb_layout.cpp): CTA k
-// produces the products of source chunk k and finishes destination chunk k,
-// bin by bin. All indices in the engine's device order.
-struct PbHost {
-    int32_t n_chunks = 0, n_bins = 0;
-    std::vector<int32_t> src_start;   // n_chunks + 1 over the source dimension
-    std::vector<int32_t> dst_start;   // n_chunks + 1 over the destination dimension
-    std::vector<int32_t> dst_bin;     // n_chunks + 1: bins of destination chunk k
-    std::vector<int32_t> bin_first;   // n_bins + 1: first destination index of each bin
-    std::vector<int32_t> dst_ptr;     // destination CSR offsets (= product places of its rows)
-    std::vector<int32_t> src_first;   // n_chunks + 1: producer-list start of each chunk
-    std::vector<uint16_t> loc;        // per producer entry: source index within its chunk
-    std::vector<float> val;           // per producer entry: the matrix value
-    std::vector<int32_t> dest;        // per producer entry: its place in the product buffer
-    std::vector<uint16_t> slot;       // per product place: its slot within its bin
-    int32_t max_src_chunk = 0, max_dst_chunk = 0, max_bin_entries = 0;
-};
-// Builds one direction (dst x src matrix with entries (dst[e], src[e], val[e]))
-// over the given chunk bounds (n_chunks + 1 each); false when the matrix does
-// not fit the format (a row longer than a bin, a source chunk above 65,535
-// indices, 2^31 or more entries).
-bool build_pb(int32_t n_dst, int32_t n_src, const std::vector<int32_t>& dst, const std::vector<int32_t>& src,
-              const std::vector<float>& val, const std::vector<int32_t>& src_start,
-              const std::vector<int32_t>& dst_start, int32_t bin_entries, PbHost& out);
-// y = M x through the layout on the host, as the device computes it.
-void pb_spmv_host(const PbHost& P, int32_t n_dst, const double* x, double* y);
-// Chunk bounds over [0, w.size()): `parts` chunks of about equal weight (w[i] + 1
-// each), cut early where a chunk reaches max_len indices.
-std::vector<int32_t> pb_split(const std::vector<int32_t>& w, int32_t parts, int32_t max_len);
-
 constexpr int kLenBits = 27;
 constexpr uint32_t kLenMask = (1u << kLenBits) - 1;
 

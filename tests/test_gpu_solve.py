@@ -6,10 +6,11 @@ numbers -- and its objective is compared with the reference CPU PDLP and the
 reference FP64 dual simplex on the same inputs (golden fixtures made by
 running the reference, tests/golden/make_golden.py). Tolerances:
   * tol 1e-6: eps_P, eps_D, eps_G <= 1e-6 (certified); the engine's own
-    eps_P/eps_D/eps_G agree with the independent check; objective within 1e-6
-    relative of the dual simplex and of the reference CPU PDLP at 1e-6. The one
-    exception is adlittle, where the reference's own PDLP at 1e-6 lands 1.54e-6
-    from the simplex: there both bounds are twice the reference's own gap;
+    eps_P/eps_D/eps_G agree with the independent check; objective within
+    2.5e-6 relative of the dual simplex (what eps_G <= 1e-6 allows, see
+    conftest.GAP_BOUND_1E6) and within 2.5e-6 plus the reference PDLP's own
+    distance from the optimum of the reference CPU PDLP's 1e-6 point; the
+    random family within 1e-6 of both;
   * tol 1e-8: objective within 1e-6 relative of the dual simplex and of the
     reference PDLP at 1e-8.
 """
@@ -18,7 +19,8 @@ import pytest
 
 import b200pdlp as B
 import oracle as O
-from conftest import OBJ_TOL, as_form, fixture_names, fixture_obj_tol, golden_index, load_fixture, random_case, rel
+from conftest import (OBJ_TOL, as_form, fixture_names, fixture_obj_tol, fixture_ref_tol, golden_index, load_fixture,
+                      random_case, rel)
 
 pytestmark = pytest.mark.gpu
 
@@ -44,11 +46,12 @@ def test_fixture_tol_1e6(name, precision):
     assert r.eps_P == pytest.approx(v["eps_P"], rel=1e-6, abs=1e-12)
     assert r.eps_D == pytest.approx(v["eps_D"], rel=1e-6, abs=1e-12)
     assert r.eps_G == pytest.approx(v["eps_G"], rel=1e-6, abs=1e-12)
-    tol_obj = fixture_obj_tol(name)
+    b_spx, b_ref = fixture_obj_tol(name), fixture_ref_tol(name)
     e_spx = rel(v["objective"], g["simplex"]["objective"])
     e_ref = rel(v["objective"], g["pdlp"]["1e-06"]["form_objective"])
-    print(f"OBJ {name} prec={precision} vs_simplex={e_spx:.2e} vs_ref_pdlp={e_ref:.2e} bound={tol_obj:.2e}")
-    assert e_spx <= tol_obj and e_ref <= tol_obj, (e_spx, e_ref, tol_obj)
+    print(f"OBJ {name} prec={precision} vs_simplex={e_spx:.2e} (bound {b_spx:.2e}) vs_ref_pdlp={e_ref:.2e} "
+          f"(bound {b_ref:.2e})")
+    assert e_spx <= b_spx and e_ref <= b_ref, (e_spx, e_ref, b_spx, b_ref)
 
 
 @pytest.mark.parametrize("name", ["afiro", "sc50a", "blend", "beaconfd", "israel", "share1b"])
