@@ -1,19 +1,20 @@
 """This engine against the reference's own plain FP64 GPU PDLP
 (gpu/pdlp_gpu_solve.cu, compiled for sm_100a into the oracle) on the same B200.
 
-The reference engine syncs the host once per attempt and runs two host
-verify() calls every 64 accepted steps, so its full solves of the large LPs
-take minutes; it is timed on two bounded samples of attempts, and its solve
-time is extrapolated as setup + attempts x (time per attempt), with the
-attempts its own algorithm needs (this engine's FP64 mode takes the
-reference's decisions, so that count is the reference's).
+The single large LP's >= 5x is measured in full, not modelled:
+tests/test_gpu_golden_large.py compares this engine's solve time with the
+reference engine's recorded full solve of the same LP (tests/golden/large.json:
+413.7 s, 143,360 attempts, on a B200). Here the batch and the served stream are
+compared with the reference engine run one LP at a time. Its full solves of
+the stream's larger LPs take minutes each, so per size class it is timed on two
+bounded samples of attempts and its solve time extrapolated as setup + attempts
+x (time per attempt), with the attempts this engine's answer took; the batch's
+sample LPs are solved in full.
 
-Targets: the 500,000 x 1,000,000 LP (8M nonzeros) solved >= 5x faster by the
-mixed-precision engine; a batch of uneven LPs >= 20x the solves/s of the
+Targets: a batch of uneven LPs and the served stream >= 20x the solves/s of the
 plain engine solving them one at a time. The measured figures are printed.
 """
 import json
-import time
 
 import numpy as np
 import pytest
@@ -35,26 +36,6 @@ def ref_time_model(P, n1, n2):
     per = (r2["seconds"] - r1["seconds"]) / (r2["iterations"] - r1["iterations"])
     setup = max(0.0, r1["seconds"] - r1["iterations"] * per)
     return setup, per
-
-
-def test_large_lp_vs_plain_fp64_gpu():
-    lp = B.gen_random_lp(500_000, 1_000_000, 8, 1, True)
-    U, S, Dr, Dc, _ = B.prepare(lp)
-    with B.Engine(U, S, Dr, Dc) as eng:
-        eng.solve(max_iterations=2000, tol=1e-6)  # warm-up
-        t0 = time.perf_counter()
-        r = eng.solve(max_iterations=2_000_000, tol=1e-6, copy_out=False)
-        ours_s = time.perf_counter() - t0
-        r64 = eng.solve(max_iterations=2_000_000, tol=1e-6, precision=B.PREC_FP64, copy_out=False)
-    assert r.converged and r64.converged
-    P = O.RefProblem.from_form(as_form(U), use_presolve=False, gpu=True)
-    setup, per = ref_time_model(P, 128, 640)
-    ref_s = setup + r64.iterations * per
-    line = {"lp": "random 500000x1000000, 8 nnz/col", "engine_s": ours_s, "engine_attempts": r.iterations,
-            "plain_fp64_gpu_s_est": ref_s, "plain_setup_s": setup, "plain_ms_per_attempt": per * 1e3,
-            "plain_attempts": r64.iterations, "speedup": ref_s / ours_s}
-    print("PLAIN_FP64_LARGE " + json.dumps(line))
-    assert ref_s / ours_s >= 5.0, line
 
 
 def test_batch_vs_plain_fp64_gpu_one_at_a_time():
