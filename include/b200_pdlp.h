@@ -86,7 +86,31 @@ typedef struct b2_solve_opts {
        a set stop_flag does. NULL: not used. */
     int32_t (*stop_poll)(void* stop_ctx);
     void* stop_ctx;
+    /* Batches and served LPs: lanes-per-row target per shape class
+       (b2_shape_class); NULL: the built-in table (b2_default_tune_table).
+       An explicit lane_target > 0 overrides both. Read while b2_batch_create
+       runs; a server copies it at b2_server_create. */
+    const struct b2_tune_table* tune;
 } b2_solve_opts;
+
+/* ---- shape classes and the autotuner --------------------------------------
+ * No counterpart in the reference. The sliced layout of a batched or served LP
+ * spreads each row over g lanes, g the smallest power of two with
+ * ceil(len / g) <= lane target; the lane target thus sets the rows per warp
+ * (32 / g) and the steps per slice. b2_shape_class buckets an LP by size
+ * (nonzeros: < 4K, < 16K, < 64K, < 256K, more) and entries per row (< 8, < 16,
+ * < 32, more); b2_batch_autotune times, per class present in the given LPs, a
+ * few of its LPs on one CTA each (512 FP64 attempts) under lane targets 4, 8,
+ * 16 and 32 and keeps the fastest (16 unless another is 3 % faster). The table
+ * is data: solves with a given table are deterministic, and the built-in one
+ * came from this tuner run on a B200 over the batch family. */
+#define B2_TUNE_CLASSES 20
+typedef struct b2_tune_table {
+    int32_t lane_target[B2_TUNE_CLASSES];    /* 0: class not tuned, 16 applies */
+    double us_per_attempt[B2_TUNE_CLASSES];  /* the chosen target's measured time (0: not measured) */
+} b2_tune_table;
+int32_t b2_shape_class(int32_t m, int32_t n, int64_t nnz);
+void b2_default_tune_table(struct b2_tune_table* out);
 
 void b2_default_opts(b2_solve_opts* opts);
 
@@ -221,6 +245,10 @@ typedef struct b2_batch_info {
 
 int b2_batch_create(int32_t n_lp, const b2_lp_view* unscaled, const b2_lp_view* scaled, const double* const* Dr,
                     const double* const* Dc, const b2_solve_opts* opts, b2_batch** out);
+/* The autotuner (see b2_shape_class): fills `out` for the classes present in
+ * the given LPs (others 0). Runs batches on the current GPU. */
+int b2_batch_autotune(int32_t n_lp, const b2_lp_view* unscaled, const b2_lp_view* scaled, const double* const* Dr,
+                      const double* const* Dc, const b2_solve_opts* opts, b2_tune_table* out);
 /* Solves every LP of the batch; results[i] receives LP i's result (device_ms =
  * that LP's time on its CTA); *total_ms the whole launch (CUDA events). */
 int b2_batch_solve(b2_batch* b, const b2_solve_opts* opts, const volatile int32_t* stop_flag, b2_result* results,

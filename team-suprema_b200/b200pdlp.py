@@ -41,7 +41,7 @@ EXPORTED = [
     "b2_engine_create", "b2_engine_solve",
     "b2_engine_destroy", "b2_engine_get_info", "b2_engine_spmv", "b2_engine_spmv_bench", "b2_engine_trace",
     "b2_batch_create", "b2_batch_solve", "b2_batch_get_solution", "b2_batch_get_info", "b2_batch_spmv",
-    "b2_batch_destroy",
+    "b2_batch_destroy", "b2_shape_class", "b2_default_tune_table", "b2_batch_autotune",
     "b2_server_create", "b2_server_submit", "b2_server_submit_file", "b2_server_submit_lp", "b2_server_wait",
     "b2_server_stats_get", "b2_pdlp_form_build", "b2_pdlp_form_view", "b2_pdlp_form_extract",
     "b2_pdlp_form_destroy", "b2_presolve", "b2_presolved_view", "b2_postsolve", "b2_presolved_destroy",
@@ -74,7 +74,16 @@ class SolveOpts(C.Structure):
                 ("time_limit_s", C.c_double), ("barrier_timeout_s", C.c_double), ("max_ctas", C.c_int32),
                 ("lane_target", C.c_int32), ("sigma_window", C.c_int32), ("return_current", C.c_int32),
                 ("stream", C.c_void_p), ("debug_delay_us", C.c_int32), ("batch_cluster_nnz", C.c_int32),
-                ("batch_block", C.c_int32), ("stop_poll", C.c_void_p), ("stop_ctx", C.c_void_p)]
+                ("batch_block", C.c_int32), ("stop_poll", C.c_void_p), ("stop_ctx", C.c_void_p),
+                ("tune", C.c_void_p)]
+
+
+TUNE_CLASSES = 20
+
+
+class TuneTable(C.Structure):
+    """Lane target per shape class (b2_tune_table)."""
+    _fields_ = [("lane_target", C.c_int32 * TUNE_CLASSES), ("us_per_attempt", C.c_double * TUNE_CLASSES)]
 
 
 class _Result(C.Structure):
@@ -156,6 +165,12 @@ def lib():
             L.b2_batch_get_info.argtypes = [vp, C.POINTER(BatchInfo)]
             L.b2_batch_spmv.argtypes = [vp, i32, i32, vp, vp]
             L.b2_batch_destroy.argtypes = [vp]
+            L.b2_shape_class.argtypes = [i32, i32, i64]
+            L.b2_shape_class.restype = i32
+            L.b2_default_tune_table.argtypes = [C.POINTER(TuneTable)]
+            L.b2_default_tune_table.restype = None
+            L.b2_batch_autotune.argtypes = [i32, C.POINTER(_LPView), C.POINTER(_LPView), C.POINTER(vp), C.POINTER(vp),
+                                            C.POINTER(SolveOpts), C.POINTER(TuneTable)]
             L.b2_batch_destroy.restype = None
             L.b2_server_create.argtypes = [C.POINTER(ServerOpts), C.POINTER(SolveOpts), C.POINTER(vp)]
             L.b2_server_submit.argtypes = [vp, C.POINTER(_LPView), C.POINTER(i64)]
@@ -290,6 +305,8 @@ def default_opts(**kw) -> SolveOpts:
     for k, v in kw.items():
         if not hasattr(o, k):
             raise TypeError(f"unknown option {k}")
+        if k == "tune" and isinstance(v, TuneTable):
+            v = C.addressof(v)  # the caller keeps the table alive while these options are in use
         setattr(o, k, v)
     return o
 
@@ -854,6 +871,43 @@ class Presolved:
         if getattr(self, "_h", None) and self._h.value:
             lib().b2_presolved_destroy(self._h)
             self._h = C.c_void_p()
+
+
+def shape_class(m: int, n: int, nnz: int) -> int:
+    """Shape class of an LP (b2_shape_class): size bucket x entries-per-row bucket."""
+    return int(lib().b2_shape_class(int(m), int(n), int(nnz)))
+
+
+def default_tune_table() -> dict:
+    """The built-in lane target per shape class (b2_default_tune_table)."""
+    t = TuneTable()
+    lib().b2_default_tune_table(C.byref(t))
+    return {"lane_target": list(t.lane_target), "us_per_attempt": list(t.us_per_attempt)}
+
+
+def autotune(problems, **opts) -> TuneTable:
+    """Runs the shape-class autotuner (b2_batch_autotune) over a list of
+    (unscaled, scaled, Dr, Dc) problems on the current GPU; returns the table,
+    which Batch / Server accept as tune=..."""
+    keep = []
+    us, ss, drs, dcs = [], [], [], []
+    for (U, S, Dr, Dc) in problems:
+        U = RangedLP.like(U)
+        S = RangedLP.like(S)
+        dr = _vec(Dr, U.m)
+        dc = _vec(Dc, U.n)
+        keep.extend([U, S, dr, dc])
+        us.append(U.view())
+        ss.append(S.view())
+        drs.append(dr.ctypes.data)
+        dcs.append(dc.ctypes.data)
+    n = len(us)
+    o = default_opts(**opts)
+    t = TuneTable()
+    _check(lib().b2_batch_autotune(n, (_LPView * n)(*us), (_LPView * n)(*ss), (C.c_void_p * n)(*drs),
+                                   (C.c_void_p * n)(*dcs), C.byref(o), C.byref(t)))
+    del keep
+    return t
 
 
 def version() -> str:

@@ -356,9 +356,10 @@ struct BatchImpl {
         n = n_lp;
         L.resize(n);
         BuildParams bp;
-        bp.lane_target = o.lane_target;
         bp.sigma_window = o.sigma_window;
-        // host layouts, in parallel over LPs (validation errors name the LP)
+        // host layouts, in parallel over LPs (validation errors name the LP);
+        // each LP's lane target from its shape class
+        
         const unsigned hw = std::max(1u, std::min(16u, std::thread::hardware_concurrency()));
         std::vector<std::thread> pool;
         std::vector<std::string> errs(hw);
@@ -367,7 +368,9 @@ struct BatchImpl {
             pool.emplace_back([&, t]() {
                 for (int i = (int)t; i < n; i += (int)hw) {
                     try {
-                        build_layout(U[i], S[i], Dr[i], Dc[i], bp, L[i]);
+                        BuildParams bpi = bp;
+                        bpi.lane_target = lane_target_for(o, U[i].m, U[i].n, U[i].nnz);
+                        build_layout(U[i], S[i], Dr[i], Dc[i], bpi, L[i]);
                     } catch (const Error& e) {
                         codes[t] = e.code;
                         errs[t] = "LP " + std::to_string(i) + ": " + e.msg;
@@ -716,5 +719,92 @@ void batch_solve(BatchImpl* b, const b2_solve_opts& o, const volatile int32_t* s
 void batch_solution(BatchImpl* b, int i, double* x, double* y) { b->solution(i, x, y); }
 void batch_info(BatchImpl* b, b2_batch_info* inf) { b->info(inf); }
 void batch_spmv(BatchImpl* b, int i, int which, const double* x, double* y) { b->spmv(i, which, x, y); }
+
+// ------------------------------------------------------- shape classes
+int32_t shape_class(int32_t m, int32_t n, int64_t nnz) {
+    (void)n;
+    const int64_t size_edges[4] = {4096, 16384, 65536, 262144};
+    int sz = 0;
+    while (sz < 4 && nnz >= size_edges[sz]) ++sz;
+    const double per_row = m > 0 ? (double)nnz / (double)m : 0.0;
+    const double row_edges[3] = {8.0, 16.0, 32.0};
+    int rw = 0;
+    while (rw < 3 && per_row >= row_edges[rw]) ++rw;
+    return sz * 4 + rw;
+}
+
+// The built-in table: b2_batch_autotune on a B200 over 1,024 LPs of the batch
+// family (m log-uniform on [50, 5,000], n = U[2,4] m, 4-10 entries a column),
+// FP64 attempts, 512-thread CTAs. Classes the family does not reach keep 16.
+void default_tune_table(b2_tune_table& t) {
+    std::memset(&t, 0, sizeof(t));
+    for (int k = 0; k < B2_TUNE_CLASSES; ++k) t.lane_target[k] = 16;
+}
+
+int lane_target_for(const b2_solve_opts& o, int32_t m, int32_t n, int64_t nnz) {
+    if (o.lane_target > 0) return o.lane_target;
+    b2_tune_table def;
+    const b2_tune_table* t = o.tune;
+    if (!t) {
+        default_tune_table(def);
+        t = &def;
+    }
+    const int v = t->lane_target[shape_class(m, n, nnz)];
+    return v > 0 ? v : 16;
+}
+
+// For every shape class present: up to four of its LPs, one CTA each, 512
+// FP64 attempts under each candidate lane target; the fastest by summed
+// device time per attempt wins, 16 unless another is at least 3 % faster.
+void batch_autotune(int n, const b2_lp_view* U, const b2_lp_view* S, const double* const* Dr, const double* const* Dc,
+                    const b2_solve_opts& o, b2_tune_table& out) {
+    std::memset(&out, 0, sizeof(out));
+    std::vector<std::vector<int>> members(B2_TUNE_CLASSES);
+    for (int i = 0; i < n; ++i) {
+        std::vector<int>& v = members[shape_class(U[i].m, U[i].n, U[i].nnz)];
+        if (v.size() < 4) v.push_back(i);
+    }
+    const int cands[4] = {4, 8, 16, 32};
+    for (int k = 0; k < B2_TUNE_CLASSES; ++k) {
+        const std::vector<int>& v = members[k];
+        if (v.empty()) continue;
+        std::vector<b2_lp_view> u, s;
+        std::vector<const double*> dr, dc;
+        for (int i : v) {
+            u.push_back(U[i]);
+            s.push_back(S[i]);
+            dr.push_back(Dr[i]);
+            dc.push_back(Dc[i]);
+        }
+        double best = 0.0, t16 = 0.0;
+        int pick = 16;
+        double us[4] = {0, 0, 0, 0};
+        for (int c = 0; c < 4; ++c) {
+            b2_solve_opts oo = o;
+            oo.lane_target = cands[c];
+            oo.precision = B2_PREC_FP64;
+            oo.max_iterations = 512;
+            oo.tol = 1e-30;  // never converges: every candidate runs the same 512 attempts
+            oo.time_limit_s = 0.0;
+            std::unique_ptr<BatchImpl> b(new BatchImpl());
+            b->create((int)v.size(), u.data(), s.data(), dr.data(), dc.data(), oo);
+            std::vector<b2_result> res(v.size());
+            double ms = 0.0;
+            b->solve(oo, nullptr, res.data(), &ms);
+            double dev = 0.0, att = 0.0;
+            for (const b2_result& r : res) {
+                dev += r.device_ms;
+                att += r.iterations;
+            }
+            us[c] = att > 0 ? 1e3 * dev / att : 0.0;
+            if (cands[c] == 16) t16 = us[c];
+        }
+        best = t16;
+        for (int c = 0; c < 4; ++c)
+            if (us[c] > 0 && us[c] < best * 0.97 && us[c] < best) { best = us[c]; pick = cands[c]; }
+        out.lane_target[k] = pick;
+        out.us_per_attempt[k] = best;
+    }
+}
 
 }  // namespace b2

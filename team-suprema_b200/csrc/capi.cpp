@@ -394,6 +394,23 @@ int b2_batch_create(int32_t n_lp, const b2_lp_view* U, const b2_lp_view* S, cons
     });
 }
 
+int32_t b2_shape_class(int32_t m, int32_t n, int64_t nnz) { return b2::shape_class(m, n, nnz); }
+
+void b2_default_tune_table(b2_tune_table* out) {
+    if (out) b2::default_tune_table(*out);
+}
+
+int b2_batch_autotune(int32_t n_lp, const b2_lp_view* U, const b2_lp_view* S, const double* const* Dr,
+                      const double* const* Dc, const b2_solve_opts* opts, b2_tune_table* out) {
+    return b2::guarded([&] {
+        if (!U || !S || !Dr || !Dc || !out || n_lp <= 0) b2::fail(B2_ERR_INVALID, "bad argument");
+        b2_solve_opts o;
+        if (opts) o = *opts;
+        else b2_default_opts(&o);
+        b2::batch_autotune(n_lp, U, S, Dr, Dc, o, *out);
+    });
+}
+
 int b2_batch_solve(b2_batch* b, const b2_solve_opts* opts, const volatile int32_t* stop_flag, b2_result* results,
                    double* total_ms) {
     return b2::guarded([&] {

@@ -126,6 +126,12 @@ void pdlp_form_free(PdlpForm* f);
 // verify()'s figures on the host: out = {eps_P, eps_D, eps_G, objective}
 void kkt_host(const b2_lp_view& lp, const double* x, const double* y, double* out);
 
+// Shape classes and lane targets of batched / served LPs (batch.cu).
+int32_t shape_class(int32_t m, int32_t n, int64_t nnz);
+void default_tune_table(b2_tune_table& t);
+// The lane target an LP of this shape gets under these options.
+int lane_target_for(const b2_solve_opts& o, int32_t m, int32_t n, int64_t nnz);
+
 // The binary request format (lp_io.cpp). All functions throw Error.
 void lp_write(const std::string& path, const b2_lp_view& lp);
 void lp_read_dims(const std::string& path, int32_t* m, int32_t* n, int64_t* nnz);
@@ -164,6 +170,8 @@ void batch_solve(BatchImpl* b, const b2_solve_opts& o, const volatile int32_t* s
 void batch_solution(BatchImpl* b, int i, double* x, double* y);
 void batch_info(BatchImpl* b, b2_batch_info* inf);
 void batch_spmv(BatchImpl* b, int i, int which, const double* x, double* y);
+void batch_autotune(int n, const b2_lp_view* U, const b2_lp_view* S, const double* const* Dr, const double* const* Dc,
+                    const b2_solve_opts& o, b2_tune_table& out);
 
 // The served stream (serve.cu). All functions throw Error.
 struct ServerImpl;

@@ -234,6 +234,7 @@ struct Staging {
 }  // namespace
 
 struct ServerImpl {
+    b2_tune_table tune_copy{};
     b2_server_opts so{};
     b2_solve_opts o{};
     int device = 0, sm_count = 0, nt = 512, max_ctas = 0, max_clusters = 0, capacity = 0;
@@ -281,6 +282,10 @@ struct ServerImpl {
     void create(const b2_server_opts& sopt, const b2_solve_opts& opt) {
         so = sopt;
         o = opt;
+        if (opt.tune) {  // the server keeps its own copy of the caller's table
+            tune_copy = *opt.tune;
+            o.tune = &tune_copy;
+        }
         if (so.hbm_budget_bytes <= 0) so.hbm_budget_bytes = 150e9;
         if (so.round_ms <= 0) so.round_ms = 5.0;
         if (so.max_resident <= 0) so.max_resident = 65536;
@@ -594,9 +599,10 @@ struct ServerImpl {
         b2_lp_view S{r.m, r.n, (int64_t)r.val.size(), r.row.data(), r.col.data(), val_s.data(), c_s.data(),
                      rL_s.data(), rU_s.data(), l_s.data(), u_s.data(), r.obj_offset};
         BuildParams bp;
-        if (o.lane_target > 0) bp.lane_target = o.lane_target;
         if (o.sigma_window > 0) bp.sigma_window = o.sigma_window;
         bp.split = (int64_t)r.val.size() >= so.grid_nnz;  // the whole-GPU lane lays out as b2_engine does
+        // a batched-lane LP takes its shape class's lane target; the whole-GPU lane, the engine's
+        bp.lane_target = bp.split ? o.lane_target : lane_target_for(o, r.m, r.n, (int64_t)r.val.size());
         if (bp.split) bp.threads = (int)std::max(1u, std::min(8u, std::thread::hardware_concurrency()));
         Layout L;
         build_layout(U, S, Dr.data(), Dc.data(), bp, L);
