@@ -11,7 +11,7 @@ def test_shape_class_buckets():
     assert B.shape_class(5000, 15000, 105_000) == 3 * 4 + 2    # 64K-256K
     assert B.shape_class(500_000, 1_000_000, 8_000_000) == 4 * 4 + 2
     assert B.shape_class(100, 100, 100) == 0                   # 1 a row
-    assert B.shape_class(10, 10, 10_000) == 2 * 4 + 3          # 1,000 a row
+    assert B.shape_class(10, 10, 10_000) == 1 * 4 + 3          # 1,000 a row, 4K-16K
     assert B.shape_class(0, 5, 0) == 0
 
 
