@@ -454,7 +454,8 @@ def batch_bench(args, world, rank, local):
     bt = B.Batch(probs)
     t_create = time.time() - t0
     info = bt.info()
-    bopts = dict(precision=prec, batch_block=args.batch_block, batch_cluster_nnz=args.batch_cluster_nnz)
+    bopts = dict(precision=prec, batch_block=args.batch_block, batch_cluster_nnz=args.batch_cluster_nnz,
+                 batch_tail_attempts=args.batch_tail_attempts)
     for _ in range(args.warmup):
         bt.solve(max_iterations=2_000_000, tol=args.tol, **bopts)
     dist_barrier(world)
@@ -810,6 +811,8 @@ def main():
     ap.add_argument("--batch-mhi", type=int, default=0, help="batch: largest m of the family (0: 5000; profiling)")
     ap.add_argument("--serve-seconds", type=float, default=0.0, help="serve: arrival window (0: workload default)")
     ap.add_argument("--round-ms", type=float, default=5.0, help="serve: device time of one batched round")
+    ap.add_argument("--batch-tail-attempts", type=int, default=0,
+                    help="batch: LPs still running at this many attempts finish on 16-CTA clusters (0: off)")
     ap.add_argument("--batch-cluster-nnz", type=int, default=0,
                     help="batch: stored entries from which an LP is solved by a cluster (0 auto, <0 never)")
     args = ap.parse_args()

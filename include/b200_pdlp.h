@@ -91,6 +91,13 @@ typedef struct b2_solve_opts {
        An explicit lane_target > 0 overrides both. Read while b2_batch_create
        runs; a server copies it at b2_server_create. */
     const struct b2_tune_table* tune;
+    /* Batches, the tail lane: > 0 -- an LP still running at this many attempts
+       yields there, and once the one-CTA launch is done the yielded LPs finish
+       on 16-CTA clusters on the whole GPU (a second launch). The switch point
+       depends on the LP alone, so answers stay deterministic, but such an LP's
+       bits differ from its solve on one CTA (the group size sets the order of
+       its reductions). <= 0: off (default). Not with batch_cluster_nnz. */
+    int32_t batch_tail_attempts;
 } b2_solve_opts;
 
 /* ---- shape classes and the autotuner --------------------------------------

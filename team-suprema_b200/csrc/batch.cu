@@ -55,6 +55,7 @@ __device__ void fill_params(KParamsBase& P, const BatchArgs& B, const LpDev& d) 
     P.debug_delay_ns = 0;
     P.trace = nullptr;
     P.trace_cap = 0;
+    P.yield_attempts = B.tail_attempts;
 }
 
 // One LP solved by a group (one CTA or one cluster): parameters into this
@@ -563,6 +564,9 @@ struct BatchImpl {
         B.stall_checks = o.stall_checks > 0 ? o.stall_checks : 32;
         B.mixed = o.precision == B2_PREC_MIXED;
         B.round_ns = 0;
+        const bool tail = o.batch_tail_attempts > 0 && large_q.empty() && shape.max_clusters_nt[ntx] > 0;
+        B.tail_attempts = tail ? o.batch_tail_attempts : 0;
+        if (tail) cuda_ok(cudaMemsetAsync(B.qstatus, 0xff, sizeof(int) * small_q.size(), st), "memset");
         *h_stop = stop_requested(o, stop_flag) ? 1 : 0;
         cuda_ok(cudaMemcpyAsync(lps_ctl(0), h.data(), sizeof(dev::Ctl) * n, cudaMemcpyHostToDevice, st), "ctl upload");
         cuda_ok(cudaMemsetAsync(B.next, 0, sizeof(unsigned), st), "memset");
@@ -594,14 +598,42 @@ struct BatchImpl {
             batch_kernel_launch(B, false, nt, ctas, st);
             last_ctas = ctas;
         }
-        cuda_ok(cudaEventRecord(ev1, st), "event");
-        for (;;) {
-            cudaError_t q = cudaEventQuery(ev1);
-            if (q == cudaSuccess) break;
-            if (q != cudaErrorNotReady) cuda_ok(q, "batched kernel");
-            if (stop_requested(o, stop_flag)) *(volatile int*)h_stop = 1;
-            std::this_thread::sleep_for(std::chrono::microseconds(20));
+        auto wait_for = [&](cudaEvent_t ev) {
+            for (;;) {
+                cudaError_t q = cudaEventQuery(ev);
+                if (q == cudaSuccess) break;
+                if (q != cudaErrorNotReady) cuda_ok(q, "batched kernel");
+                if (stop_requested(o, stop_flag)) *(volatile int*)h_stop = 1;
+                std::this_thread::sleep_for(std::chrono::microseconds(20));
+            }
+        };
+        if (tail) {
+            // the tail lane: LPs that yielded at batch_tail_attempts finish on
+            // clusters of 16 CTAs, on the whole GPU, once the one-CTA launch is done
+            cuda_ok(cudaEventRecord(ev1, st), "event");
+            wait_for(ev1);
+            std::vector<int> qs(small_q.size());
+            if (!qs.empty())
+                cuda_ok(cudaMemcpy(qs.data(), B.qstatus, sizeof(int) * qs.size(), cudaMemcpyDeviceToHost), "status");
+            std::vector<int> yielded;
+            for (size_t k = 0; k < qs.size(); ++k)
+                if (qs[k] == 0) yielded.push_back(small_q[k]);
+            if (!yielded.empty() && !*h_stop) {
+                cuda_ok(cudaMemcpyAsync((void*)B.order_large, yielded.data(), sizeof(int) * yielded.size(),
+                                        cudaMemcpyHostToDevice, st), "queue");
+                cuda_ok(cudaMemsetAsync(B.next_large, 0, sizeof(unsigned), st), "memset");
+                dev::BatchArgs Bt = B;
+                Bt.n_inst = 0;
+                Bt.n_large = (int)yielded.size();
+                Bt.tail_attempts = 0;
+                const int ncl = std::min((int)yielded.size(), shape.max_clusters_nt[ntx]);
+                batch_kernel_launch(Bt, true, nt, ncl, st);
+                last_ctas = std::max(last_ctas, ncl * dev::kMaxCluster);
+                for (int i : yielded) last_cluster[i] = 1;
+            }
         }
+        cuda_ok(cudaEventRecord(ev1, st), "event");
+        wait_for(ev1);
         float ms = 0.0f;
         cuda_ok(cudaEventElapsedTime(&ms, ev0, ev1), "elapsed");
         if (total_ms) *total_ms = ms;

@@ -28,6 +28,7 @@ struct BatchArgs {
     unsigned long long round_ns;      // groups yield this long after the launch starts; 0: never
     double tol, switch_tol, time_limit_ns;
     int max_iterations, check_every, stall_checks, mixed;
+    int tail_attempts;                // > 0: LPs yield from this attempt on (the tail lane finishes them)
 };
 
 }  // namespace dev

@@ -130,6 +130,9 @@ struct KParamsBase {
     unsigned long long debug_delay_ns;  // test hook: the group's first CTA arrives late at its first barrier
     double* trace;                      // per-check records (kTraceFields doubles), may be null
     int trace_cap;
+    // > 0: the solve yields at its first attempt boundary from this attempt on
+    // (a batch's tail lane; the point depends on the LP alone, not on timing)
+    int yield_attempts;
 };
 
 template <class T>
@@ -1110,6 +1113,7 @@ __device__ bool solve_body(const KParams<T>& P, const Group& g) {
                     else if (__ldcg(&g.bcast[1]) != 0.0) s.stop_req = B2_EXIT_TIME_LIMIT;
                 }
                 if (ypoll && __ldcg(&g.bcast[3]) != 0.0) s.yield_req = 1;
+                if (P.yield_attempts > 0 && s.attempts >= P.yield_attempts) s.yield_req = 1;
                 s_flag[0] = (s.last_accepted && (s.accepted % P.check_every) == 0) || s.attempts >= P.max_iterations;
             }
             __syncthreads();

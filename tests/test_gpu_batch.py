@@ -122,3 +122,32 @@ def test_cluster_path_certified():
         one.solve(max_iterations=500000, tol=1e-6, batch_cluster_nnz=1500)
         x1, _ = one.solution(0)
     np.testing.assert_array_equal(x0, x1)
+
+
+def test_tail_lane_certified_deterministic_and_untouched_below_the_switch():
+    """The tail lane (batch_tail_attempts): LPs still running at 300 attempts
+    yield there and finish on 16-CTA clusters in a second launch. Every answer
+    is certified; two runs give the same bits; LPs that finish before the
+    switch are bit-identical to the batch without a tail lane."""
+    names, probs = fixture_problems()
+    keys = sorted(G["random"].keys())
+    for k in keys:
+        _, U, S, Dr, Dc, _ = random_case(k)
+        probs.append((U, S, Dr, Dc))
+    runs = []
+    for tail in (300, 300, 0):
+        with B.Batch(probs) as bt:
+            res, _ = bt.solve(max_iterations=500000, tol=1e-6, batch_tail_attempts=tail)
+            runs.append((res, [bt.solution(i) for i in range(len(probs))]))
+    (r1, s1), (r2, s2), (r0, s0) = runs
+    moved = [i for i, r in enumerate(r1) if r["group_ctas"] > 1]
+    assert moved and len(moved) < len(probs)
+    for i, (U, S, Dr, Dc) in enumerate(probs):
+        assert r1[i]["converged"], (i, r1[i])
+        assert r1[i]["iterations"] == r2[i]["iterations"]
+        np.testing.assert_array_equal(s1[i][0], s2[i][0])
+        v = O.verify(as_form(U), *s1[i])
+        assert max(v["eps_P"], v["eps_D"], v["eps_G"]) <= 1e-6 * (1 + 1e-9)
+        if i not in moved:
+            assert r1[i]["iterations"] == r0[i]["iterations"] <= 300 + 64
+            np.testing.assert_array_equal(s1[i][0], s0[i][0])
