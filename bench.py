@@ -770,7 +770,7 @@ def profile_mode(args):
     lp = make_lp(B, args.workload)
     U, S, Dr, Dc, _ = B.prepare(lp)
     prec = B.PREC_MIXED if args.precision == "mixed" else B.PREC_FP64
-    with B.Engine(U, S, Dr, Dc) as eng:
+    with B.Engine(U, S, Dr, Dc, long_rows=args.long_rows) as eng:
         if args.mode == "spmv":
             a = eng.spmv_bench(0, prec, args.reps)
             t = eng.spmv_bench(1, prec, args.reps)
@@ -803,6 +803,8 @@ def main():
     ap.add_argument("--mode", default="bench", choices=["bench", "spmv", "solve"],
                     help="spmv / solve: one short run of that kernel for profiling (ncu), no JSON line")
     ap.add_argument("--max-attempts", type=int, default=256, help="--mode solve: attempt limit")
+    ap.add_argument("--long-rows", type=int, default=0, choices=[0, 1],
+                    help="--mode solve/spmv: long rows by the sector cost model (0) or the length rule (1)")
     ap.add_argument("--switch-tol", type=float, default=0.0,
                     help="--mode solve, mixed precision: KKT level of the FP32 -> FP64 hand-over (0: default)")
     ap.add_argument("--reps", type=int, default=1, help="--mode spmv: timed launches per product")

@@ -98,6 +98,10 @@ typedef struct b2_solve_opts {
        bits differ from its solve on one CTA (the group size sets the order of
        its reductions). <= 0: off (default). Not with batch_cluster_nnz. */
     int32_t batch_tail_attempts;
+    /* Whole-GPU engine, rows of 256+ entries: 0 -- the lanes per row that touch
+       the fewest memory sectors (a cost model over the rows' own columns);
+       1 -- the length rule of all other rows (lane_target). Read at create. */
+    int32_t long_rows;
 } b2_solve_opts;
 
 /* ---- shape classes and the autotuner --------------------------------------

@@ -75,7 +75,7 @@ class SolveOpts(C.Structure):
                 ("lane_target", C.c_int32), ("sigma_window", C.c_int32), ("return_current", C.c_int32),
                 ("stream", C.c_void_p), ("debug_delay_us", C.c_int32), ("batch_cluster_nnz", C.c_int32),
                 ("batch_block", C.c_int32), ("stop_poll", C.c_void_p), ("stop_ctx", C.c_void_p),
-                ("tune", C.c_void_p), ("batch_tail_attempts", C.c_int32)]
+                ("tune", C.c_void_p), ("batch_tail_attempts", C.c_int32), ("long_rows", C.c_int32)]
 
 
 TUNE_CLASSES = 20

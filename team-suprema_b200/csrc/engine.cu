@@ -207,6 +207,7 @@ struct EngineImpl {
         bp.lane_target = o.lane_target;
         bp.sigma_window = o.sigma_window;
         bp.split = true;  // the whole GPU works on this LP: tune and split long rows
+        if (o.long_rows == 1) bp.tune_len = INT32_MAX;  // the length rule for every row
         bp.threads = (int)std::max(1u, std::min(8u, std::thread::hardware_concurrency()));
         build_layout(U, S, Dr, Dc, bp, L);
         create_device();
