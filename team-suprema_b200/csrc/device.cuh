@@ -418,33 +418,75 @@ __device__ __forceinline__ AccT slice_dot(const SellDev& S, const V* vbase, int4
     return acc;
 }
 
-// Sum of a lane's partials of a split group in segment order; the loads are
-// issued 16 at a time (the adds stay one chain, so the order is fixed).
+// Split groups add their segments' partial sums in two levels: subgroups of
+// kSubSeg consecutive segments are added in segment order, then the subgroup
+// totals in subgroup order. The order is fixed by the layout, so every run
+// gives the same bits, and the owner of the rows waits for a few subgroup
+// totals instead of adding up to 255 partials in one chain.
+constexpr int kSubSeg = 16;
+// arrival counters per split group: [0] subgroup leaders, [1 + k] members of subgroup k
+constexpr int kSegCounters = 1 + (255 + kSubSeg - 1) / kSubSeg;
+
+template <class AccT>
+__device__ __forceinline__ AccT sum_sub(const double* part, int first, int count, int lane) {
+    // loads issued 8 at a time; the adds stay one chain in segment order
+    AccT s = AccT(0);
+    for (int h = 0; h < count; h += 8) {
+        double v[8];
+#pragma unroll
+        for (int k = 0; k < 8; ++k) v[k] = h + k < count ? __ldcg(part + (first + h + k) * 32 + lane) : 0.0;
+#pragma unroll
+        for (int k = 0; k < 8; ++k)
+            if (h + k < count) s += (AccT)v[k];
+    }
+    return s;
+}
+
+// The two-level sum of all `segments` partials of a lane (the order seg_finish uses).
 template <class AccT>
 __device__ __forceinline__ AccT sum_partials(const double* part, int segments, int lane) {
     AccT tot = AccT(0);
-    int t = 0;
-    for (; t + 16 <= segments; t += 16) {
-        double v[16];
-#pragma unroll
-        for (int k = 0; k < 16; ++k) v[k] = __ldcg(part + (t + k) * 32 + lane);
-#pragma unroll
-        for (int k = 0; k < 16; ++k) tot += (AccT)v[k];
+    for (int f = 0; f < segments; f += kSubSeg) {
+        const AccT sub = sum_sub<AccT>(part, f, min(kSubSeg, segments - f), lane);
+        tot = f == 0 ? sub : tot + (AccT)(double)sub;
     }
-    for (; t < segments; ++t) tot += (AccT)__ldcg(part + t * 32 + lane);
     return tot;
+}
+
+// Lane 0 waits (bounded) until *cnt reaches want, then zeroes it for the next
+// product; the warp learns whether the wait succeeded.
+__device__ __forceinline__ bool seg_wait(unsigned* cnt, unsigned want, const Group& g, int lane) {
+    int ok = 1;
+    if (lane == 0 && want > 0) {
+        const unsigned long long t0 = gtimer();
+        unsigned spins = 0;
+        for (;;) {
+            unsigned cur;
+            asm volatile("ld.acquire.gpu.u32 %0,[%1];" : "=r"(cur) : "l"(cnt) : "memory");
+            if (cur == want) break;
+            if ((++spins & 63u) == 0) {
+                if (*(volatile int*)g.abort || gtimer() - t0 > g.timeout_ns) { atomicExch(g.abort, 1); ok = 0; break; }
+            }
+        }
+        if (ok) *cnt = 0u;  // all have arrived: ready for the next product
+    }
+    ok = __shfl_sync(0xffffffffu, ok, 0);
+    __syncwarp();
+    return ok != 0;
 }
 
 // A split slice is one of `segments` consecutive slice records over the same
 // rows, each covering a range of steps (slice.w = group + 1 | segment << 24;
 // 0 for an unsplit slice); only the whole-GPU layout has them. Every segment
-// publishes its lanes' partial sums and counts itself in; the warp of segment
-// 0 owns the rows: it waits (bounded) until the others have arrived, adds the
-// partials in segment order and alone runs the rows' epilogue, so the sums,
-// and which CTA's reductions the rows land in, never depend on timing.
-// Waits cannot form a cycle: segment 0 waits only on the next segments - 1
-// slice records, and the launch keeps segments <= the group's warp count, so
-// none of them is a later slice of the waiting warp itself.
+// publishes its lanes' partial sums; a member counts itself in with its
+// subgroup's leader (the subgroup's first segment), which waits (bounded) for
+// the subgroup, adds its partials in order and leaves the subtotal in its own
+// slot; the warp of segment 0 (leader of subgroup 0) owns the rows: it waits
+// for the other leaders, adds the subtotals in order and alone runs the rows'
+// epilogue, so the sums, and which CTA's reductions the rows land in, never
+// depend on timing. Waits cannot form a cycle: a warp waits only on later
+// slice records of its own group, and the launch keeps segments <= the
+// group's warp count, so none of them is a later slice of the waiting warp.
 // Returns whether this warp holds complete row sums in `acc`.
 template <int GK, class AccT>
 __device__ __forceinline__ bool seg_finish(const SellDev& S, int4 sl, int lane, AccT& acc, const Group& g) {
@@ -452,56 +494,56 @@ __device__ __forceinline__ bool seg_finish(const SellDev& S, int4 sl, int lane, 
     const int grp = (sl.w & 0xFFFFFF) - 1, q = (int)((unsigned)sl.w >> 24);
     const int2 info = __ldg(S.seg + grp);
     double* part = S.seg_part + (size_t)info.y * 32;
+    unsigned* cnt = S.seg_cnt + (size_t)grp * kSegCounters;
+    const int sub = q / kSubSeg, lead = sub * kSubSeg;
+    const int members = min(kSubSeg, info.x - lead);
     __stcg(part + q * 32 + lane, (double)acc);
     __threadfence();
     __syncwarp();
-    if (q != 0) {
-        if (lane == 0) atomicAdd(S.seg_cnt + grp, 1u);
+    if (q != lead) {
+        if (lane == 0) atomicAdd(cnt + 1 + sub, 1u);
         return false;
     }
-    int ok = 1;
-    if (lane == 0) {
-        const unsigned want = (unsigned)(info.x - 1);
-        const unsigned long long t0 = gtimer();
-        unsigned spins = 0;
-        for (;;) {
-            unsigned cur;
-            asm volatile("ld.acquire.gpu.u32 %0,[%1];" : "=r"(cur) : "l"(S.seg_cnt + grp) : "memory");
-            if (cur == want) break;
-            if ((++spins & 63u) == 0) {
-                if (*(volatile int*)g.abort || gtimer() - t0 > g.timeout_ns) { atomicExch(g.abort, 1); ok = 0; break; }
-            }
-        }
-        if (ok) S.seg_cnt[grp] = 0u;  // all have arrived: ready for the next product
-    }
-    ok = __shfl_sync(0xffffffffu, ok, 0);
-    __syncwarp();
-    if (!ok) return false;  // the group's next barrier reports the abort
+    if (!seg_wait(cnt + 1 + sub, (unsigned)(members - 1), g, lane)) return false;  // abort: the next barrier reports it
     __threadfence();
-    acc = sum_partials<AccT>(part, info.x, lane);
+    const AccT subtotal = sum_sub<AccT>(part, lead, members, lane);
+    if (q != 0) {
+        __stcg(part + q * 32 + lane, (double)subtotal);
+        __threadfence();
+        __syncwarp();
+        if (lane == 0) atomicAdd(cnt, 1u);
+        return false;
+    }
+    const int nsub = (info.x + kSubSeg - 1) / kSubSeg;
+    if (!seg_wait(cnt, (unsigned)(nsub - 1), g, lane)) return false;
+    __threadfence();
+    AccT tot = subtotal;
+    for (int k = 1; k < nsub; ++k) tot += (AccT)__ldcg(part + k * kSubSeg * 32 + lane);
+    acc = tot;
     return true;
 }
 
 // The same for a product with no reductions behind it (the standalone SpMV):
-// whichever warp completes the group adds the partials in segment order, so
-// nobody waits and the sums are still the same bits.
+// whichever warp completes the group adds the partials in the same two-level
+// order, so nobody waits and the sums are the same bits.
 template <class AccT>
 __device__ __forceinline__ bool seg_finish_last(const SellDev& S, int4 sl, int lane, AccT& acc) {
     if (sl.w == 0) return true;
     const int grp = (sl.w & 0xFFFFFF) - 1, q = (int)((unsigned)sl.w >> 24);
     const int2 info = __ldg(S.seg + grp);
     double* part = S.seg_part + (size_t)info.y * 32;
+    unsigned* cnt = S.seg_cnt + (size_t)grp * kSegCounters;
     __stcg(part + q * 32 + lane, (double)acc);
     __threadfence();
     __syncwarp();
     unsigned last = 0;
-    if (lane == 0) last = atomicAdd(S.seg_cnt + grp, 1u) == (unsigned)(info.x - 1) ? 1u : 0u;
+    if (lane == 0) last = atomicAdd(cnt, 1u) == (unsigned)(info.x - 1) ? 1u : 0u;
     last = __shfl_sync(0xffffffffu, last, 0);
     __syncwarp();
     if (!last) return false;
     __threadfence();
     acc = sum_partials<AccT>(part, info.x, lane);
-    if (lane == 0) S.seg_cnt[grp] = 0u;  // the next product comes after this kernel
+    if (lane == 0) *cnt = 0u;  // the next product comes after this kernel
     return true;
 }
 

@@ -167,7 +167,8 @@ struct EngineImpl {
     void clear_seg_counters(cudaStream_t st) {
         for (const dev::SellDev* d : {&A, &AT})
             if (d->seg_cnt)
-                cuda_ok(cudaMemsetAsync(d->seg_cnt, 0, sizeof(unsigned) * (size_t)(d == &A ? L.A : L.AT).n_groups(), st),
+                cuda_ok(cudaMemsetAsync(d->seg_cnt, 0,
+                                        sizeof(unsigned) * dev::kSegCounters * (size_t)(d == &A ? L.A : L.AT).n_groups(), st),
                         "memset");
     }
 
@@ -182,8 +183,9 @@ struct EngineImpl {
         if (S.n_groups() > 0) {
             d.seg = reinterpret_cast<const int2*>(up(S.seg));
             d.seg_part = alloc<double>((size_t)S.seg_slots * 32);
-            unsigned* cnt = alloc<unsigned>((size_t)S.n_groups());
-            cuda_ok(cudaMemsetAsync(cnt, 0, sizeof(unsigned) * (size_t)S.n_groups(), stream), "memset");
+            const size_t ncnt = (size_t)dev::kSegCounters * (size_t)S.n_groups();
+            unsigned* cnt = alloc<unsigned>(ncnt);
+            cuda_ok(cudaMemsetAsync(cnt, 0, sizeof(unsigned) * ncnt, stream), "memset");
             d.seg_cnt = cnt;
         }
         return d;
