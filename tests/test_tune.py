@@ -19,3 +19,4 @@ def test_default_table_is_complete():
     t = B.default_tune_table()
     assert len(t["lane_target"]) == B.TUNE_CLASSES
     assert all(v in (4, 8, 16, 32) for v in t["lane_target"])
+    assert t["lane_target"][B.shape_class(3000, 9000, 54_000)] == 32  # measured on a B200: 16+ a row, 16K-64K
