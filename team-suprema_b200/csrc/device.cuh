@@ -442,12 +442,20 @@ __device__ __forceinline__ AccT sum_sub(const double* part, int first, int count
     return s;
 }
 
-// The two-level sum of all `segments` partials of a lane (the order seg_finish uses).
+// The two-level sum of all `segments` partials of a lane (the order seg_finish
+// uses), for the standalone product: a whole subgroup's loads in flight at once.
 template <class AccT>
 __device__ __forceinline__ AccT sum_partials(const double* part, int segments, int lane) {
     AccT tot = AccT(0);
     for (int f = 0; f < segments; f += kSubSeg) {
-        const AccT sub = sum_sub<AccT>(part, f, min(kSubSeg, segments - f), lane);
+        const int count = min(kSubSeg, segments - f);
+        double v[kSubSeg];
+#pragma unroll
+        for (int k = 0; k < kSubSeg; ++k) v[k] = k < count ? __ldcg(part + (f + k) * 32 + lane) : 0.0;
+        AccT sub = AccT(0);
+#pragma unroll
+        for (int k = 0; k < kSubSeg; ++k)
+            if (k < count) sub += (AccT)v[k];
         tot = f == 0 ? sub : tot + (AccT)(double)sub;
     }
     return tot;
