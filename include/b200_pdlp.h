@@ -400,6 +400,21 @@ void b2_pool_destroy(b2_pool* p);
 int b2_layout_digest(const b2_lp_view* unscaled_form, const b2_lp_view* scaled_form, const double* Dr,
                      const double* Dc, int32_t threads, int32_t whole_gpu, uint64_t* digest);
 
+/* No counterpart in the reference. The shape of that layout, for callers
+ * sizing or tuning it (no GPU): slice records of A and A^T (a split slice
+ * counts once per segment), stored entries with padding, split groups, and
+ * dense-run records (whole_gpu = 1 only), whose columns are an arithmetic run
+ * c0 + k * ks + lane: the engine computes their addresses instead of reading a
+ * column stream. */
+typedef struct b2_layout_stats {
+    int64_t a_slices, at_slices;
+    int64_t a_padded, at_padded;
+    int64_t a_groups, at_groups;
+    int64_t a_dense, at_dense;
+} b2_layout_stats;
+int b2_layout_get_stats(const b2_lp_view* unscaled_form, const b2_lp_view* scaled_form, const double* Dr,
+                        const double* Dc, int32_t whole_gpu, b2_layout_stats* out);
+
 /* ---- host-side preparation (product side, no GPU needed) ---------------- */
 
 /* Ruiz (ruiz_passes) + Pock-Chambolle alpha=1 scaling, as scale() in

@@ -46,7 +46,7 @@ EXPORTED = [
     "b2_server_stats_get", "b2_pdlp_form_build", "b2_pdlp_form_view", "b2_pdlp_form_extract",
     "b2_pdlp_form_destroy", "b2_presolve", "b2_presolved_view", "b2_postsolve", "b2_presolved_destroy",
     "b2_server_destroy", "b2_lp_write", "b2_lp_read_dims", "b2_lp_read",
-    "b2_layout_digest", "b2_request_work", "b2_shard_plan", "b2_pool_create", "b2_pool_submit", "b2_pool_submit_file",
+    "b2_layout_digest", "b2_layout_get_stats", "b2_request_work", "b2_shard_plan", "b2_pool_create", "b2_pool_submit", "b2_pool_submit_file",
     "b2_pool_wait", "b2_pool_stats_get", "b2_pool_destroy",
     "b2_scale", "b2_scale_gpu",
     "b2_gen_random_lp", "b2_gen_transport", "b2_last_error", "b2_version",
@@ -127,6 +127,12 @@ class EngineInfo(C.Structure):
                 ("sm_count", C.c_int32), ("device_bytes", C.c_int64)]
 
 
+class LayoutStats(C.Structure):
+    _fields_ = [("a_slices", C.c_int64), ("at_slices", C.c_int64), ("a_padded", C.c_int64),
+                ("at_padded", C.c_int64), ("a_groups", C.c_int64), ("at_groups", C.c_int64),
+                ("a_dense", C.c_int64), ("at_dense", C.c_int64)]
+
+
 _lib = None
 _lib_lock = threading.Lock()
 
@@ -194,6 +200,8 @@ def lib():
             L.b2_server_wait.argtypes = [vp, i64, f64, vp, vp, C.POINTER(_Result), C.POINTER(RequestInfo)]
             L.b2_server_stats_get.argtypes = [vp, C.POINTER(ServerStats)]
             L.b2_server_destroy.argtypes = [vp]
+            L.b2_layout_get_stats.argtypes = [C.POINTER(_LPView), C.POINTER(_LPView), vp, vp, i32,
+                                              C.POINTER(LayoutStats)]
             L.b2_layout_digest.argtypes = [C.POINTER(_LPView), C.POINTER(_LPView), vp, vp, i32, i32,
                                            C.POINTER(C.c_uint64)]
             L.b2_request_work.argtypes = [i32, i32, i64]
@@ -605,6 +613,19 @@ def layout_digest(unscaled_form: RangedLP, scaled_form: RangedLP, Dr, Dc, thread
     _check(lib().b2_layout_digest(C.byref(U.view()), C.byref(S.view()), _ptr(dr), _ptr(dc), int(threads),
                                   int(bool(whole_gpu)), C.byref(d)))
     return d.value
+
+
+def layout_stats(unscaled_form: RangedLP, scaled_form: RangedLP, Dr, Dc, whole_gpu: bool = True) -> dict:
+    """Shape of the device layout (b2_layout_get_stats; no GPU): slice
+    records, stored entries, split groups and dense-run records of A and A^T."""
+    U = RangedLP.like(unscaled_form)
+    S = RangedLP.like(scaled_form)
+    dr = _vec(Dr, U.m)
+    dc = _vec(Dc, U.n)
+    st = LayoutStats()
+    _check(lib().b2_layout_get_stats(C.byref(U.view()), C.byref(S.view()), _ptr(dr), _ptr(dc),
+                                     int(bool(whole_gpu)), C.byref(st)))
+    return {k: getattr(st, k) for k, _ in LayoutStats._fields_}
 
 
 # --------------------------------------------------- shares over several GPUs

@@ -320,6 +320,26 @@ int b2_layout_digest(const b2_lp_view* U, const b2_lp_view* S, const double* Dr,
     });
 }
 
+int b2_layout_get_stats(const b2_lp_view* U, const b2_lp_view* S, const double* Dr, const double* Dc,
+                        int32_t whole_gpu, b2_layout_stats* out) {
+    return b2::guarded([&] {
+        if (!U || !S || !out) b2::fail(B2_ERR_INVALID, "null argument");
+        b2::BuildParams bp;
+        bp.split = whole_gpu != 0;
+        bp.threads = (int)std::max(1u, std::min(8u, std::thread::hardware_concurrency()));
+        b2::Layout L;
+        b2::build_layout(*U, *S, Dr, Dc, bp, L);
+        out->a_slices = L.A.n_slices();
+        out->at_slices = L.AT.n_slices();
+        out->a_padded = L.A.padded;
+        out->at_padded = L.AT.padded;
+        out->a_groups = L.A.n_groups();
+        out->at_groups = L.AT.n_groups();
+        out->a_dense = L.A.n_dense;
+        out->at_dense = L.AT.n_dense;
+    });
+}
+
 int64_t b2_request_work(int32_t m, int32_t n, int64_t nnz) { return b2::request_work(m, n, nnz); }
 
 int b2_shard_plan(const int64_t* work, int64_t count, int32_t parts, int32_t online, int32_t* rank_of) {

@@ -81,6 +81,9 @@ struct SellDev {
     const int2* seg;
     double* seg_part;
     unsigned* seg_cnt;
+    // dense runs (whole-GPU engine only): per slice record {c0, ks} when lane
+    // l of step k holds column c0 + k * ks + l, else {-1, 0}; null: none
+    const int2* aff;
 };
 
 template <class T>
@@ -215,6 +218,54 @@ __device__ __forceinline__ T ld_it(const T* p) {
     return __ldcg(p);
 }
 
+// One-dimensional bulk copy (TMA engine) from this GPU's global memory into
+// this CTA's shared memory, completed on an mbarrier: the issuing thread
+// announces the bytes (arrive.expect_tx) and the copy counts them off. Both
+// addresses 16-byte aligned, bytes a multiple of 16. No multicast.
+__device__ __forceinline__ uint32_t smem_addr(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+__device__ __forceinline__ void mbar_init(unsigned long long* bar, unsigned count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(bar)), "r"(count) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+__device__ __forceinline__ void bulk_to_smem(void* dst, const void* src, uint32_t bytes, unsigned long long* bar) {
+    // the source was written through the generic proxy (other SMs, ordered by
+    // the grid barrier) and the destination last read through it: order both
+    // before the async-proxy copy
+    asm volatile("fence.proxy.async;" ::: "memory");
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)), "r"(bytes) : "memory");
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                     smem_addr(dst)),
+                 "l"((unsigned long long)__cvta_generic_to_global(src)), "r"(bytes), "r"(smem_addr(bar))
+                 : "memory");
+}
+__device__ __forceinline__ bool mbar_done(unsigned long long* bar, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\tselp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(smem_addr(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+// Waits (bounded) for the copy of phase `parity`; past the limit it raises
+// `abort` and gives the copy, which still targets this CTA's shared memory, a
+// second bounded wait before the caller goes on to the barrier that ends it.
+__device__ __forceinline__ void mbar_wait(unsigned long long* bar, uint32_t parity, int* abort,
+                                          unsigned long long timeout_ns) {
+    if (mbar_done(bar, parity)) return;
+    const unsigned long long t0 = gtimer();
+    unsigned spins = 0;
+    while (!mbar_done(bar, parity)) {
+        if ((++spins & 63u) == 0 && gtimer() - t0 > timeout_ns) {
+            atomicExch(abort, 1);
+            const unsigned long long t1 = gtimer();
+            while (!mbar_done(bar, parity) && gtimer() - t1 < timeout_ns) {
+            }
+            return;
+        }
+    }
+}
+
 template <class V>
 __device__ __forceinline__ const V* vals(const SellDev& S);
 template <>
@@ -332,6 +383,24 @@ __device__ __forceinline__ void cta_partial(double (&v)[NV], const Group& g, int
 }
 
 // After a barrier: every CTA sums the CTA partials of one slot in CTA order.
+// One lane's share of a sum over the group's CTAs: p[b * stride] for b = lane,
+// lane + 32, ... < size, added in that order. The loads of up to 320 CTAs are
+// issued before the first add, so the sum costs one L2 round trip, not one
+// per CTA.
+__device__ __forceinline__ double lane_parts(const double* p, int size, size_t stride, int lane) {
+    constexpr int kIn = 10;
+    double s = 0.0;
+    for (int b0 = lane; b0 < size; b0 += 32 * kIn) {
+        double v[kIn];
+#pragma unroll
+        for (int q = 0; q < kIn; ++q) v[q] = b0 + 32 * q < size ? __ldcg(p + (size_t)(b0 + 32 * q) * stride) : 0.0;
+#pragma unroll
+        for (int q = 0; q < kIn; ++q)
+            if (b0 + 32 * q < size) s += v[q];
+    }
+    return s;
+}
+
 template <int NV, int GK>
 __device__ __forceinline__ void group_totals(const Group& g, int slot, double* s_tot) {
     if (GK == GK_CTA) {
@@ -341,8 +410,7 @@ __device__ __forceinline__ void group_totals(const Group& g, int slot, double* s
     }
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     for (int k = warp; k < NV; k += (int)(blockDim.x >> 5)) {
-        double s = 0.0;
-        for (int b = lane; b < g.size; b += 32) s += __ldcg(&g.part[((size_t)slot * g.size + b) * kPartStride + k]);
+        double s = lane_parts(g.part + (size_t)slot * g.size * kPartStride + k, g.size, kPartStride, lane);
         s = warp_total(s);
         if (lane == 0) s_tot[k] = s;
     }
@@ -365,8 +433,7 @@ __device__ __forceinline__ void step_totals(const Group& g, double* s_tot) {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     if (warp < 3) {
         const int slot = warp < 2 ? SLOT_A : SLOT_X, k = warp < 2 ? warp : 0;
-        double s = 0.0;
-        for (int b = lane; b < g.size; b += 32) s += __ldcg(&g.part[((size_t)slot * g.size + b) * kPartStride + k]);
+        double s = lane_parts(g.part + (size_t)slot * g.size * kPartStride + k, g.size, kPartStride, lane);
         s = warp_total(s);
         if (lane == 0) s_tot[warp] = s;
     }
@@ -381,9 +448,11 @@ __device__ __forceinline__ void step_totals(const Group& g, double* s_tot) {
 #endif
 constexpr int kUnroll = B2_SLICE_UNROLL;
 
-template <int GK, class AccT, class V, class XT>
+// LOCAL: x is a copy in this CTA's shared memory (plain loads).
+template <int GK, class AccT, class V, class XT, bool LOCAL = false>
 __device__ __forceinline__ AccT slice_dot(const SellDev& S, const V* vbase, int4 sl, int lane, const XT* x) {
     constexpr bool KEEP = GK == GK_CTA;
+    constexpr int GX = LOCAL ? GK_CTA : GK;
     const uint32_t len = (uint32_t)sl.y & kLenMask;
     const int lg = (int)((uint32_t)sl.y >> kLenBits);
     const size_t base = (size_t)(uint32_t)sl.z * 32u + (size_t)lane;
@@ -403,16 +472,56 @@ __device__ __forceinline__ AccT slice_dot(const SellDev& S, const V* vbase, int4
             vv[q] = ld_mat<KEEP>(vp + 32 * q);
         }
 #pragma unroll
-        for (int q = 0; q < kUnroll; ++q) xx[q] = (AccT)ld_it<GK>(x + cc[q]);
+        for (int q = 0; q < kUnroll; ++q) xx[q] = (AccT)ld_it<GX>(x + cc[q]);
 #pragma unroll
         for (int q = 0; q < kUnroll; ++q) acc = fma((AccT)vv[q], xx[q], acc);
         cp += 32 * kUnroll;
         vp += 32 * kUnroll;
     }
     for (; k < len; ++k) {
-        acc = fma((AccT)ld_mat<KEEP>(vp), (AccT)ld_it<GK>(x + ld_mat<KEEP>(cp)), acc);
+        acc = fma((AccT)ld_mat<KEEP>(vp), (AccT)ld_it<GX>(x + ld_mat<KEEP>(cp)), acc);
         cp += 32;
         vp += 32;
+    }
+    for (int o = (1 << lg) >> 1; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
+    return acc;
+}
+
+// The same product for a dense-run record (columns c0 + k * ks + lane): the
+// gather addresses are computed, not read, so every step's value and x loads
+// are independent and kDenseUnroll steps are in flight at once. The stored
+// column stream holds the same indices; padding positions gather a column in
+// range with a zero value, as the stream's padding does, so the sums are
+// those of slice_dot.
+constexpr int kDenseUnroll = 8;
+template <int GK, class AccT, class V, class XT, bool LOCAL = false>
+__device__ __forceinline__ AccT slice_dot_dense(const V* vbase, int4 sl, int2 af, int lane, const XT* x) {
+    constexpr bool KEEP = GK == GK_CTA;
+    constexpr int GX = LOCAL ? GK_CTA : GK;
+    const uint32_t len = (uint32_t)sl.y & kLenMask;
+    const int lg = (int)((uint32_t)sl.y >> kLenBits);
+    const V* vp = vbase + (size_t)(uint32_t)sl.z * 32u + (size_t)lane;
+    const XT* xp = x + (int64_t)af.x + lane;
+    const int64_t ks = af.y;
+    AccT acc = AccT(0);
+    uint32_t k = 0;
+    for (; k + kDenseUnroll <= len; k += kDenseUnroll) {
+        V vv[kDenseUnroll];
+        AccT xx[kDenseUnroll];
+#pragma unroll
+        for (int q = 0; q < kDenseUnroll; ++q) {
+            vv[q] = ld_mat<KEEP>(vp + 32 * q);
+            xx[q] = (AccT)ld_it<GX>(xp + (int64_t)q * ks);
+        }
+#pragma unroll
+        for (int q = 0; q < kDenseUnroll; ++q) acc = fma((AccT)vv[q], xx[q], acc);
+        vp += 32 * kDenseUnroll;
+        xp += (int64_t)kDenseUnroll * ks;
+    }
+    for (; k < len; ++k) {
+        acc = fma((AccT)ld_mat<KEEP>(vp), (AccT)ld_it<GX>(xp), acc);
+        vp += 32;
+        xp += ks;
     }
     for (int o = (1 << lg) >> 1; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
     return acc;
@@ -653,20 +762,22 @@ __device__ void pass_rows_step(const KParams<T>& P, const Ctl& c, const Group& g
     const V* vb = vals<V>(P.A);
     for (int s = g.gw; s < P.A.n_slices; s += g.nw) {
         const int4 sl = __ldg(P.A.slice + s);
+        const int2 af = P.A.aff ? __ldg(P.A.aff + s) : make_int2(-1, 0);
         const int lg = (int)((uint32_t)sl.y >> kLenBits);
         const int row = sl.x + (lane >> lg);
         const bool lead = (lane & ((1 << lg) - 1)) == 0 && row < P.m;
         // the epilogue's operands are loaded before the product, so their
         // latency hides behind its gathers
         T yv = T(0), axv = T(0);
-        double w = 0.0, brow = 0.0;
+        double w = 0.0, brow = 0.0, ys = 0.0;
         if (lead) {
             yv = ld_it<GK>(y + row);
             axv = ld_it<GK>(ax + row);
             w = __ldg(P.dr2 + row);
             brow = __ldg(P.b + row);
+            if (pend != 0.0) ys = P.ysum[row];
         }
-        T acc = slice_dot<GK, T, V, T>(P.A, vb, sl, lane, xn);
+        T acc = af.x >= 0 ? slice_dot_dense<GK, T, V, T>(vb, sl, af, lane, xn) : slice_dot<GK, T, V, T>(P.A, vb, sl, lane, xn);
         if (!seg_finish<GK, T>(P.A, sl, lane, acc, g)) continue;
         if (lead) {
             const double aw = fabs(w);
@@ -679,7 +790,7 @@ __device__ void pass_rows_step(const KParams<T>& P, const Ctl& c, const Group& g
             const double d = (double)nt - (double)yv;
             v[0] += d * d / aw;
             v[1] += d * ((double)acc - (double)axv);
-            if (pend != 0.0) P.ysum[row] += pend * (double)yv;
+            if (pend != 0.0) P.ysum[row] = ys + pend * (double)yv;
         }
     }
 }
@@ -697,23 +808,28 @@ __device__ void pass_cols_step(const KParams<T>& P, const Ctl& c, const Group& g
         const V* vb = vals<V>(P.AT);
         for (int s = g.gw; s < P.AT.n_slices; s += g.nw) {
             const int4 sl = __ldg(P.AT.slice + s);
+            const int2 af = P.AT.aff ? __ldg(P.AT.aff + s) : make_int2(-1, 0);
             const int lg = (int)((uint32_t)sl.y >> kLenBits);
             const int j = sl.x + (lane >> lg);
             const bool lead = (lane & ((1 << lg) - 1)) == 0 && j < P.n;
             // the primal step's operands are loaded before the product
             T xv = T(0);
-            double w = 1.0, cj = 0.0, lj = 0.0, uj = 0.0;
+            double w = 1.0, cj = 0.0, lj = 0.0, uj = 0.0, xs = 0.0;
             if (lead) {
                 xv = ld_it<GK>(x + j);
                 w = __ldg(P.dc2 + j);
                 cj = __ldg(P.c + j);
                 col_bounds(P, j, lj, uj);
+                if (pend != 0.0) xs = P.xsum[j];
             }
-            T acc = slice_dot<GK, T, V, T>(P.AT, vb, sl, lane, y);
+            T acc = af.x >= 0 ? (sy ? slice_dot_dense<GK, T, V, T, true>(vb, sl, af, lane, y)
+                                    : slice_dot_dense<GK, T, V, T>(vb, sl, af, lane, y))
+                              : (sy ? slice_dot<GK, T, V, T, true>(P.AT, vb, sl, lane, y)
+                                    : slice_dot<GK, T, V, T>(P.AT, vb, sl, lane, y));
             if (!seg_finish<GK, T>(P.AT, sl, lane, acc, g)) continue;
             if (lead) {
                 aty[j] = acc;
-                if (pend != 0.0) P.xsum[j] += pend * (double)xv;
+                if (pend != 0.0) P.xsum[j] = xs + pend * (double)xv;
                 primal_col_w<T>(j, xv, (double)acc, tau, xn, dx2, sx, w, cj, lj, uj);
             }
         }
@@ -966,8 +1082,7 @@ __device__ bool yield_state(const KParamsBase& P, Ctl& s, const Group& g) {
     if (GK == GK_CTA) {
         if (threadIdx.x == 0) s_carry = cta_sum(g, SLOT_X, 0);
     } else if (threadIdx.x < 32) {
-        double v = 0.0;
-        for (int b = threadIdx.x; b < g.size; b += 32) v += __ldcg(&g.part[((size_t)SLOT_X * g.size + b) * kPartStride]);
+        double v = lane_parts(g.part + (size_t)SLOT_X * g.size * kPartStride, g.size, kPartStride, threadIdx.x);
         v = warp_total(v);
         if (threadIdx.x == 0) s_carry = v;
     }
@@ -1016,6 +1131,20 @@ __device__ bool solve_body(const KParams<T>& P, const Group& g) {
     if (STAGE && GK == GK_CTA && g.svec && ((size_t)P.n + (size_t)P.m) * sizeof(T) <= (size_t)g.svec_bytes) {
         sx = reinterpret_cast<T*>(g.svec);
         sy = sx + P.n;
+    }
+    // The whole grid, an LP with few rows: every CTA takes a copy of y' into
+    // its shared memory right after the rows barrier (one bulk copy, while the
+    // step totals are formed), and the columns pass gathers y' from there.
+    __shared__ __align__(8) unsigned long long s_ybar;
+    T* ys = nullptr;
+    uint32_t ybar_parity = 0;
+    const uint32_t ybytes = (uint32_t)(((size_t)P.m * sizeof(T) + 15) & ~(size_t)15);
+    if (GK == GK_GRID && g.svec && P.m > 0 && ybytes <= (uint32_t)g.svec_bytes &&
+        ((reinterpret_cast<uintptr_t>(P.it.y[0]) | reinterpret_cast<uintptr_t>(P.it.y[1]) |
+          reinterpret_cast<uintptr_t>(g.svec)) & 15u) == 0) {
+        ys = reinterpret_cast<T*>(g.svec);
+        if (tid == 0) mbar_init(&s_ybar, 1);
+        __syncthreads();
     }
 
     // ---------------------------------------------------------- start-up
@@ -1131,6 +1260,7 @@ __device__ bool solve_body(const KParams<T>& P, const Group& g) {
                 if (ypoll) g.bcast[3] = gtimer() >= g.yield_at ? 1.0 : 0.0;
             }
             if (!group_sync<GK>(g)) return false;
+            if (ys && tid == 0) bulk_to_smem(ys, P.it.y[1 - s.yi], ybytes, &s_ybar);
             step_totals<GK>(g, s_tot);
             if (tid == 0) {
                 // adaptive step size (pdlp_algo.hpp:107-131)
@@ -1165,13 +1295,17 @@ __device__ bool solve_body(const KParams<T>& P, const Group& g) {
                 if (ypoll && __ldcg(&g.bcast[3]) != 0.0) s.yield_req = 1;
                 if (P.yield_attempts > 0 && s.attempts >= P.yield_attempts) s.yield_req = 1;
                 s_flag[0] = (s.last_accepted && (s.accepted % P.check_every) == 0) || s.attempts >= P.max_iterations;
+                if (ys) {
+                    mbar_wait(&s_ybar, ybar_parity, g.abort, g.timeout_ns);
+                    ybar_parity ^= 1u;
+                }
             }
             __syncthreads();
             const bool check_due = s_flag[0] != 0;
             // ---- cols pass: A^T y' (if accepted) + next primal step ----
             {
                 double dx2[1] = {0.0};
-                pass_cols_step<GK, T, V>(P, s, g, lane, dx2[0], sx, sy);
+                pass_cols_step<GK, T, V>(P, s, g, lane, dx2[0], sx, GK == GK_GRID ? ys : sy);
                 cta_partial<1, GK>(dx2, g, SLOT_X, s_red);
             }
             if (tid == 0) {
@@ -1256,7 +1390,9 @@ __global__ void __launch_bounds__(256) k_spmv(SellDev S, const XT* x, AccT* y) {
     const V* vb = vals<V>(S);
     for (int s = gw; s < S.n_slices; s += nw) {
         const int4 sl = __ldg(S.slice + s);
-        AccT acc = slice_dot<GK_GRID, AccT, V, XT>(S, vb, sl, lane, x);
+        const int2 af = S.aff ? __ldg(S.aff + s) : make_int2(-1, 0);
+        AccT acc = af.x >= 0 ? slice_dot_dense<GK_GRID, AccT, V, XT>(vb, sl, af, lane, x)
+                             : slice_dot<GK_GRID, AccT, V, XT>(S, vb, sl, lane, x);
         if (!seg_finish_last<AccT>(S, sl, lane, acc)) continue;
         const int lg = (int)((uint32_t)sl.y >> kLenBits);
         const int r = sl.x + (lane >> lg);

@@ -28,8 +28,12 @@ struct GridArgs {
     int* abort;
     unsigned long long timeout_ns;
     unsigned long long yield_ns;  // the solve yields this long after the launch starts; 0: never
-    int svec_bytes;               // one-CTA launch: dynamic shared memory for staged x' / y'
+    int svec_bytes;               // dynamic shared memory: the one-CTA launch's staged x' / y', the grid's y'
 };
+
+// y' staged per CTA for the grid kernel's columns pass: LPs whose y' fits in
+// this much shared memory (12,288 rows in FP32, 6,144 in FP64)
+constexpr size_t kYStageMax = 48 * 1024;
 
 template <class T, class V>
 __global__ void __launch_bounds__(kBlock, 2) k_pdlp(const KParams<T> P, const GridArgs ga) {
@@ -47,6 +51,9 @@ __global__ void __launch_bounds__(kBlock, 2) k_pdlp(const KParams<T> P, const Gr
     g.timeout_ns = ga.timeout_ns;
     g.spart = nullptr;
     if (ga.yield_ns) g.yield_at = gtimer() + ga.yield_ns;  // read on CTA 0 only
+    extern __shared__ __align__(16) unsigned char s_vec[];
+    g.svec = ga.svec_bytes > 0 ? s_vec : nullptr;
+    g.svec_bytes = ga.svec_bytes;
     solve_body<GK_GRID, T, V>(P, g);
 }
 
@@ -130,6 +137,7 @@ struct EngineImpl {
     int* h_stop = nullptr;   // pinned, mapped
     int* d_stop = nullptr;
     int max_ctas = 0;
+    int ystage_f = 0, ystage_d = 0;  // grid kernel's dynamic shared memory for y' (FP32 / FP64 iterates); 0: off
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
 
     cudaMemPool_t mpool = nullptr;
@@ -180,6 +188,7 @@ struct EngineImpl {
         d.col = up(S.col);
         d.v32 = up(S.val32);
         d.v64 = S.val64.empty() ? nullptr : up(S.val64);
+        d.aff = S.aff.empty() ? nullptr : reinterpret_cast<const int2*>(up(S.aff));
         if (S.n_groups() > 0) {
             d.seg = reinterpret_cast<const int2*>(up(S.seg));
             d.seg_part = alloc<double>((size_t)S.seg_slots * 32);
@@ -194,7 +203,8 @@ struct EngineImpl {
     template <class T>
     void alloc_bufs(dev::Bufs<T>& B) {
         for (auto& p : B.x) p = alloc<T>(L.n);
-        for (auto& p : B.y) p = alloc<T>(L.m);
+        // rounded up to 4 entries: the grid kernel's bulk copy of y' moves whole 16-byte units
+        for (auto& p : B.y) p = alloc<T>(((size_t)L.m + 3) / 4 * 4);
         for (auto& p : B.ax) p = alloc<T>(L.m);
         for (auto& p : B.aty) p = alloc<T>(L.n);
         B.x_last = alloc<T>(L.n);
@@ -254,6 +264,25 @@ struct EngineImpl {
         int per_sm = std::min(occ[0], std::min(occ[1], occ[2]));
         if (per_sm < 1) fail(B2_ERR_CUDA, "persistent kernel does not fit on an SM");
         max_ctas = per_sm * sm_count;
+        // y' staging (few rows): kept for a precision only if the grid keeps per_sm CTAs per SM
+        auto stage = [&](const void* fn, size_t elem) -> int {
+            const size_t bytes = ((size_t)L.m * elem + 15) / 16 * 16;
+            if (L.m == 0 || bytes > dev::kYStageMax) return 0;
+            if (cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes) != cudaSuccess) {
+                cudaGetLastError();
+                return 0;
+            }
+            int o = 0;
+            if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o, fn, dev::kBlock, bytes) != cudaSuccess) {
+                cudaGetLastError();
+                return 0;
+            }
+            return o >= per_sm ? (int)bytes : 0;
+        };
+        ystage_f = stage((const void*)dev::k_pdlp<float, float>, sizeof(float));
+        const int d1 = stage((const void*)dev::k_pdlp<double, float>, sizeof(double));
+        const int d2 = stage((const void*)dev::k_pdlp<double, double>, sizeof(double));
+        ystage_d = d1 > 0 && d2 > 0 ? d1 : 0;
         part = alloc<double>((size_t)dev::NSLOTS * max_ctas * dev::kPartStride);
         cuda_ok(cudaDeviceSynchronize(), "create");
     }
@@ -331,8 +360,11 @@ struct EngineImpl {
             cuda_ok(cudaGetLastError(), "k_pdlp_cta");
             return;
         }
-        void* args[] = {(void*)&P, (void*)&ga};
-        cuda_ok(cudaLaunchCooperativeKernel((const void*)dev::k_pdlp<T, V>, dim3(ctas), dim3(dev::kBlock), args, 0, st),
+        dev::GridArgs gg = ga;
+        gg.svec_bytes = sizeof(T) == 4 ? ystage_f : ystage_d;
+        void* args[] = {(void*)&P, (void*)&gg};
+        cuda_ok(cudaLaunchCooperativeKernel((const void*)dev::k_pdlp<T, V>, dim3(ctas), dim3(dev::kBlock), args,
+                                            (size_t)gg.svec_bytes, st),
                 "cudaLaunchCooperativeKernel");
     }
 

@@ -262,6 +262,8 @@ void build_sell(const std::vector<int64_t>& ptr, const std::vector<int32_t>& idx
     // over the same rows and storage
     const int64_t split_at = bp.split ? std::max(1, bp.split_steps) : INT64_MAX;
     S.slice.reserve(shapes.size() * 4);
+    std::vector<std::pair<int32_t, int64_t>> rec;  // slice record -> (shape, first step)
+    rec.reserve(shapes.size());
     for (size_t s = 0; s < shapes.size(); ++s) {
         const Shape& sh = shapes[s];
         if (sh.len > split_at) {
@@ -275,12 +277,14 @@ void build_sell(const std::vector<int64_t>& ptr, const std::vector<int32_t>& idx
             S.seg_max = std::max<int32_t>(S.seg_max, (int32_t)q_count);
             for (int64_t q = 0; q < q_count; ++q) {
                 const int64_t l0 = q * seg_steps, l1 = std::min(sh.len, l0 + seg_steps);
+                rec.emplace_back((int32_t)s, l0);
                 S.slice.push_back(sh.row0);
                 S.slice.push_back((int32_t)((uint32_t)(l1 - l0) | ((uint32_t)sh.lg << kLenBits)));
                 S.slice.push_back((int32_t)(uint32_t)(sh.blk + l0));
                 S.slice.push_back((int32_t)((uint32_t)(group + 1) | ((uint32_t)q << 24)));
             }
         } else {
+            rec.emplace_back((int32_t)s, 0);
             S.slice.push_back(sh.row0);
             S.slice.push_back((int32_t)((uint32_t)sh.len | ((uint32_t)sh.lg << kLenBits)));
             S.slice.push_back((int32_t)(uint32_t)sh.blk);
@@ -325,6 +329,46 @@ void build_sell(const std::vector<int64_t>& ptr, const std::vector<int32_t>& idx
         }
         for (auto& th : pool) th.join();
     }
+    if (!bp.split) return;
+    // dense runs: each record is checked on its own; most fail on the first
+    // lanes, and a record that passes is read once more in full
+    S.aff.assign(rec.size() * 2, 0);
+    S.n_dense = 0;
+    for (size_t r = 0; r < rec.size(); ++r) {
+        S.aff[2 * r] = -1;
+        const Shape& sh = shapes[(size_t)rec[r].first];
+        const int64_t l0 = rec[r].second;
+        const int64_t len = (int64_t)((uint32_t)S.slice[4 * r + 1] & kLenMask);
+        const int64_t blk0 = sh.blk + l0;
+        const int g = 1 << sh.lg;
+        // stored entries of each lane: a row of e entries gives lane sub of it
+        // ceil((e - sub) / g) of them
+        int64_t cnt[32];
+        for (int lane = 0; lane < 32; ++lane) {
+            const int32_t rl = lane / g, sub = lane % g;
+            cnt[lane] = 0;
+            if (rl < sh.nrows) {
+                const int32_t row = perm[sh.row0 + rl];
+                const int64_t e = ptr[row + 1] - ptr[row];
+                cnt[lane] = e > sub ? (e - sub + g - 1) / g : 0;
+            }
+        }
+        if (len < 1 || cnt[0] <= l0 || (len > 1 && cnt[0] <= l0 + 1)) continue;
+        const int64_t c0 = S.col[(size_t)(blk0 * 32)];
+        const int64_t ks = len > 1 ? (int64_t)S.col[(size_t)((blk0 + 1) * 32)] - c0 : 0;
+        bool ok = ks >= INT32_MIN && ks <= INT32_MAX;
+        for (int64_t k = 0; k < len && ok; ++k)
+            for (int lane = 0; lane < 32 && ok; ++lane) {
+                const int64_t want = c0 + k * ks + lane;
+                if (want < 0 || want >= (int64_t)S.n_cols) ok = false;
+                else if (l0 + k < cnt[lane] && (int64_t)S.col[(size_t)((blk0 + k) * 32 + lane)] != want) ok = false;
+            }
+        if (!ok) continue;
+        S.aff[2 * r] = (int32_t)c0;
+        S.aff[2 * r + 1] = (int32_t)ks;
+        ++S.n_dense;
+    }
+    if (S.n_dense == 0) S.aff.clear();
 }
 
 double finite_inf_norm(const double* v, int64_t len) {
@@ -479,7 +523,7 @@ uint64_t layout_digest(const Layout& L) {
     auto sell = [&](const SellHost& S) {
         mix(&S.n_rows, sizeof(S.n_rows));
         mix(&S.n_cols, sizeof(S.n_cols));
-        vec(S.slice); vec(S.col); vec(S.val32); vec(S.val64); vec(S.seg);
+        vec(S.slice); vec(S.col); vec(S.val32); vec(S.val64); vec(S.seg); vec(S.aff);
         mix(&S.padded, sizeof(S.padded));
         mix(&S.seg_slots, sizeof(S.seg_slots));
         mix(&S.seg_max, sizeof(S.seg_max));

@@ -44,6 +44,12 @@ struct SellHost {
     std::vector<int32_t> seg;
     int64_t seg_slots = 0;            // segments in all groups (32 partial sums each)
     int32_t seg_max = 0;              // most segments in one group
+    // dense runs (whole-GPU layout): per slice record {c0, ks} when lane l
+    // of step k holds column c0 + k * ks + l for every stored entry (and
+    // that index is a column for every padding entry), else {-1, 0}; empty
+    // when no record is one
+    std::vector<int32_t> aff;
+    int64_t n_dense = 0;
     int64_t n_slices() const { return (int64_t)slice.size() / 4; }
     int64_t n_groups() const { return (int64_t)seg.size() / 2; }
 };

@@ -166,3 +166,44 @@ def test_layout_errors_name_the_first_bad_entry_at_any_thread_count():
     with pytest.raises(B.B2Error) as e:
         B.layout_digest(V, S, Dr, Dc, threads=8)
     assert e.value.code == B.B2_ERR_NONFINITE and "entry 7" in str(e.value)
+
+
+def test_dense_run_records_of_the_whole_gpu_layout():
+    """b2_layout_get_stats: on the 2,000 x 500 transportation LP nearly every
+    slice record of A is a dense run (source rows: 500 consecutive arcs; sink
+    rows: 32 consecutive sinks a warp, one source a step), none of A^T is, and
+    a random LP has none; the batch layout never marks any."""
+    U, S, Dr, Dc, _ = B.prepare(B.gen_transport(2000, 500, 1))
+    st = B.layout_stats(U, S, Dr, Dc)
+    assert st["a_slices"] == 4109 and st["a_groups"] == 17
+    assert st["a_dense"] >= 4000, st
+    assert st["at_dense"] == 0
+    assert B.layout_stats(U, S, Dr, Dc, whole_gpu=False)["a_dense"] == 0
+    U, S, Dr, Dc, _ = B.prepare(B.gen_random_lp(2000, 4000, 8, 3, True))
+    st = B.layout_stats(U, S, Dr, Dc)
+    assert st["a_dense"] == 0 and st["at_dense"] == 0
+
+
+def test_dense_run_needs_every_stored_column_on_the_run():
+    """One dense row of 4,096 columns is one long dense run (split into
+    segments, each a dense record). The layout keeps a row's entries in their
+    input order, so two swapped entries take their segment off the run, and a
+    shuffled row has no dense record at all."""
+    n = 4096
+
+    def one_row(cols):
+        row = np.zeros(n, dtype=np.int64)
+        lp = B.RangedLP(1, n, row, np.asarray(cols), np.ones(n), np.ones(n), np.array([1.0]), np.array([1.0]),
+                        np.zeros(n), np.full(n, 10.0))
+        U, S, Dr, Dc, _ = B.prepare(lp)
+        return B.layout_stats(U, S, Dr, Dc)
+
+    st = one_row(np.arange(n))
+    assert st["a_dense"] == st["a_slices"] > 1, st
+    perm = np.arange(n)
+    perm[[100, 101]] = perm[[101, 100]]
+    st2 = one_row(perm)
+    assert st2["a_slices"] == st["a_slices"] and st2["a_dense"] == st["a_dense"] - 1, st2
+    rng = np.random.default_rng(0)
+    st3 = one_row(rng.permutation(n))
+    assert st3["a_dense"] == 0, st3
