@@ -194,15 +194,30 @@ void build_sell(const std::vector<int64_t>& ptr, const std::vector<int32_t>& idx
     struct Shape { int32_t row0, nrows, lg; int64_t len, blk; };
     std::vector<Shape> shapes;
     int64_t blk = 0;
-    auto shape_of = [&](int32_t i, int g, int32_t& nr, int64_t& len) {
-        nr = std::min<int32_t>(32 / g, rows - i);
+    // A slice does not run on into the next sigma window: rows are sorted
+    // longest first inside a window, so such a slice would take the next
+    // window's longest row as its length (padding every shorter row up to it,
+    // and splitting the slice once it is longer than split_steps). A slice
+    // always covers 32 / g rows (the device derives a lane's row from that;
+    // only the matrix's last slice may hold fewer), so a slice that would
+    // cross the window's end takes more lanes per row instead: the largest
+    // power of two of rows that still fits.
+    const int window = bp.sigma_window > 0 ? bp.sigma_window : 1024;
+    auto shape_of = [&](int32_t i, int& g, int32_t& nr, int64_t& len) {
+        const int64_t wend = ((int64_t)i / window + 1) * window;
+        if (wend < rows && wend - i < 32 / g) {
+            int64_t p = 1;
+            while (p * 2 <= wend - i) p *= 2;
+            g = (int)(32 / p);
+        }
+        nr = (int32_t)std::min<int64_t>(32 / g, rows - i);
+        if (nr != 32 / g && i + nr != rows) fail(B2_ERR_INVALID, "sliced layout: a slice short of rows inside the matrix");
         int64_t lmax = 0;
         for (int32_t t = 0; t < nr; ++t) lmax = std::max<int64_t>(lmax, ptr[perm[i + t] + 1] - ptr[perm[i + t]]);
         len = (lmax + g - 1) / g;
     };
     // the tuned choice is kept for a shape class: rows of the same length in
     // the same sigma window
-    const int window = bp.sigma_window > 0 ? bp.sigma_window : 1024;
     int64_t class_len = -1, class_win = -1;
     int class_g = 0;
     for (int32_t i = 0; i < rows;) {
@@ -229,12 +244,13 @@ void build_sell(const std::vector<int64_t>& ptr, const std::vector<int32_t>& idx
             double best = base * 0.8;
             int best_g = g;
             for (int cg = 1; cg <= 32; cg <<= 1) {
-                if (cg == g) continue;
+                int eg = cg;  // the lanes per row the slice gets (more at a window's end)
                 int32_t cnr = 0;
                 int64_t clen = 0;
-                shape_of(i, cg, cnr, clen);
-                const double c = slice_cost(ptr, idx, perm, inv_col, i, cnr, cg, clen) / entries(i, cnr);
-                if (c < best) { best = c; best_g = cg; }
+                shape_of(i, eg, cnr, clen);
+                if (eg == g) continue;
+                const double c = slice_cost(ptr, idx, perm, inv_col, i, cnr, eg, clen) / entries(i, cnr);
+                if (c < best) { best = c; best_g = eg; }
             }
             if (best_g != g) {
                 g = best_g;

@@ -207,3 +207,14 @@ def test_dense_run_needs_every_stored_column_on_the_run():
     rng = np.random.default_rng(0)
     st3 = one_row(rng.permutation(n))
     assert st3["a_dense"] == 0, st3
+
+
+def test_slices_stay_inside_sigma_windows():
+    """Rows are sorted longest first inside each sigma window; a slice that
+    ran on into the next window would take that window's longest row as its
+    length. The layout widens such a slice's lanes per row instead, so a
+    random LP of short rows has no split (overlong) slices at all."""
+    U, S, Dr, Dc, _ = B.prepare(B.gen_random_lp(20000, 40000, 8, 1, True))
+    st = B.layout_stats(U, S, Dr, Dc)
+    assert st["a_groups"] == 0 and st["at_groups"] == 0, st
+    assert st["a_padded"] < 1.04 * U.nnz, st
