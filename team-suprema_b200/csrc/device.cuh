@@ -1382,9 +1382,11 @@ __device__ bool solve_body(const KParams<T>& P, const Group& g) {
 }
 
 // Standalone SpMV of a sliced matrix (y = M x), for b2_engine_spmv and the
-// bandwidth benchmark; the same slice_dot the solver uses.
+// bandwidth benchmark; the same slice products the solver uses. The FP32
+// product stays within 32 registers so that eight 256-thread CTAs fit on an
+// SM (the launch is 8 CTAs per SM: one wave).
 template <class AccT, class V, class XT>
-__global__ void __launch_bounds__(256) k_spmv(SellDev S, const XT* x, AccT* y) {
+__global__ void __launch_bounds__(256, sizeof(AccT) == 4 ? 8 : 6) k_spmv(SellDev S, const XT* x, AccT* y) {
     const int lane = threadIdx.x & 31;
     const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, nw = (gridDim.x * blockDim.x) >> 5;
     const V* vb = vals<V>(S);
