@@ -50,7 +50,7 @@ WORKLOADS = {
 # and with FP64 iterates (`bench.py --mode solve --max-attempts 256`). A profiler cannot run
 # inside the timed region, so the roofline's `traffic` is this capture scaled by the attempts
 # of each timed launch, and the line labels it so.
-TRAFFIC_PER_ATTEMPT = {"large": (139.6e6, 170.2e6)}
+TRAFFIC_PER_ATTEMPT = {"large": (137.0e6, 184.3e6)}
 
 
 def describe(name, count=0, seconds=0.0, world=1):
