@@ -136,6 +136,13 @@ struct KParamsBase {
     // > 0: the solve yields at its first attempt boundary from this attempt on
     // (a batch's tail lane; the point depends on the LP alone, not on timing)
     int yield_attempts;
+    // whole-grid kernel: the slice records of A (a_) and A^T (t_), with their
+    // dense-run pairs, again in the order of a work-balanced schedule over the
+    // grid's warps; warp w runs records [start[w], start[w + 1]). Null:
+    // round-robin over the matrices' own record order.
+    const int4 *a_wslice, *t_wslice;
+    const int2 *a_waff, *t_waff;
+    const int *a_wstart, *t_wstart;
 };
 
 template <class T>
@@ -760,9 +767,7 @@ __device__ void pass_rows_step(const KParams<T>& P, const Ctl& c, const Group& g
     T* axn = P.it.ax[c.ax_nxt];
     const double sigma = c.eta * c.omega, pend = c.pend_y;
     const V* vb = vals<V>(P.A);
-    for (int s = g.gw; s < P.A.n_slices; s += g.nw) {
-        const int4 sl = __ldg(P.A.slice + s);
-        const int2 af = P.A.aff ? __ldg(P.A.aff + s) : make_int2(-1, 0);
+    auto one = [&](const int4 sl, const int2 af) {
         const int lg = (int)((uint32_t)sl.y >> kLenBits);
         const int row = sl.x + (lane >> lg);
         const bool lead = (lane & ((1 << lg) - 1)) == 0 && row < P.m;
@@ -778,7 +783,7 @@ __device__ void pass_rows_step(const KParams<T>& P, const Ctl& c, const Group& g
             if (pend != 0.0) ys = P.ysum[row];
         }
         T acc = af.x >= 0 ? slice_dot_dense<GK, T, V, T>(vb, sl, af, lane, xn) : slice_dot<GK, T, V, T>(P.A, vb, sl, lane, xn);
-        if (!seg_finish<GK, T>(P.A, sl, lane, acc, g)) continue;
+        if (!seg_finish<GK, T>(P.A, sl, lane, acc, g)) return;
         if (lead) {
             const double aw = fabs(w);
             double nv = (double)yv + sigma * aw * (brow - (2.0 * (double)acc - (double)axv));
@@ -792,6 +797,15 @@ __device__ void pass_rows_step(const KParams<T>& P, const Ctl& c, const Group& g
             v[1] += d * ((double)acc - (double)axv);
             if (pend != 0.0) P.ysum[row] = ys + pend * (double)yv;
         }
+    };
+    if (GK == GK_GRID && P.a_wstart) {
+        // the whole grid: this warp's range of the work-balanced schedule
+        const int s1 = __ldg(P.a_wstart + g.gw + 1);
+        for (int s = __ldg(P.a_wstart + g.gw); s < s1; ++s)
+            one(__ldg(P.a_wslice + s), P.a_waff ? __ldg(P.a_waff + s) : make_int2(-1, 0));
+    } else {
+        for (int s = g.gw; s < P.A.n_slices; s += g.nw)
+            one(__ldg(P.A.slice + s), P.A.aff ? __ldg(P.A.aff + s) : make_int2(-1, 0));
     }
 }
 
@@ -806,9 +820,7 @@ __device__ void pass_cols_step(const KParams<T>& P, const Ctl& c, const Group& g
     if (c.last_accepted) {
         const T* y = sy ? sy : P.it.y[c.yi];
         const V* vb = vals<V>(P.AT);
-        for (int s = g.gw; s < P.AT.n_slices; s += g.nw) {
-            const int4 sl = __ldg(P.AT.slice + s);
-            const int2 af = P.AT.aff ? __ldg(P.AT.aff + s) : make_int2(-1, 0);
+        auto one = [&](const int4 sl, const int2 af) {
             const int lg = (int)((uint32_t)sl.y >> kLenBits);
             const int j = sl.x + (lane >> lg);
             const bool lead = (lane & ((1 << lg) - 1)) == 0 && j < P.n;
@@ -826,12 +838,21 @@ __device__ void pass_cols_step(const KParams<T>& P, const Ctl& c, const Group& g
                                     : slice_dot_dense<GK, T, V, T>(vb, sl, af, lane, y))
                               : (sy ? slice_dot<GK, T, V, T, true>(P.AT, vb, sl, lane, y)
                                     : slice_dot<GK, T, V, T>(P.AT, vb, sl, lane, y));
-            if (!seg_finish<GK, T>(P.AT, sl, lane, acc, g)) continue;
+            if (!seg_finish<GK, T>(P.AT, sl, lane, acc, g)) return;
             if (lead) {
                 aty[j] = acc;
                 if (pend != 0.0) P.xsum[j] = xs + pend * (double)xv;
                 primal_col_w<T>(j, xv, (double)acc, tau, xn, dx2, sx, w, cj, lj, uj);
             }
+        };
+        if (GK == GK_GRID && P.t_wstart) {
+            // the whole grid: this warp's range of the work-balanced schedule
+            const int s1 = __ldg(P.t_wstart + g.gw + 1);
+            for (int s = __ldg(P.t_wstart + g.gw); s < s1; ++s)
+                one(__ldg(P.t_wslice + s), P.t_waff ? __ldg(P.t_waff + s) : make_int2(-1, 0));
+        } else {
+            for (int s = g.gw; s < P.AT.n_slices; s += g.nw)
+                one(__ldg(P.AT.slice + s), P.AT.aff ? __ldg(P.AT.aff + s) : make_int2(-1, 0));
         }
     } else {
         for (int j = g.gt; j < P.n; j += g.nt)

@@ -10,7 +10,10 @@
 #include <cstdio>
 #include <cstring>
 #include <limits>
+#include <map>
 #include <memory>
+#include <numeric>
+#include <queue>
 #include <string>
 #include <thread>
 #include <vector>
@@ -168,6 +171,99 @@ struct EngineImpl {
         if (ev0) cudaEventDestroy(ev0);
         if (ev1) cudaEventDestroy(ev1);
         if (stream) cudaStreamDestroy(stream);
+    }
+
+    // Work-balanced order of the slice records over the grid's warps, for the
+    // whole-grid kernel's rows and columns passes: the records, costliest
+    // first (unroll rounds of their steps plus a fixed share), each go to the
+    // least-loaded warp (ties: the lowest warp), so that no warp holds a much
+    // longer chain of records than the average. A warp's records then run in
+    // an order that keeps split groups free of cycles of waits: records that
+    // wait for nothing (unsplit slices, subgroup members) first, then
+    // subgroup leaders, then group owners, each in record order. A leader
+    // waits only for members and an owner only for members and leaders, so
+    // every wait ends. Deterministic: a function of the layout and the grid.
+    struct SchedDev {
+        const int4* slice = nullptr;
+        const int2* aff = nullptr;
+        const int* start = nullptr;
+    };
+    struct Sched {
+        SchedDev a, at;
+    };
+    std::map<int, Sched> scheds;  // by CTA count of the launch
+
+    SchedDev build_sched(const SellHost& S, int nw) {
+        SchedDev d;
+        const int64_t n = S.n_slices();
+        if (n == 0 || nw <= 1) return d;
+        std::vector<int64_t> cost((size_t)n);
+        for (int64_t r = 0; r < n; ++r) {
+            const int64_t len = (int64_t)((uint32_t)S.slice[(size_t)(4 * r + 1)] & kLenMask);
+            const bool dense = !S.aff.empty() && S.aff[(size_t)(2 * r)] >= 0;
+            const int64_t u = dense ? dev::kDenseUnroll : dev::kUnroll;
+            cost[(size_t)r] = (len + u - 1) / u + 2;
+        }
+        std::vector<int32_t> ord((size_t)n);
+        std::iota(ord.begin(), ord.end(), 0);
+        std::stable_sort(ord.begin(), ord.end(), [&](int32_t a, int32_t b) { return cost[(size_t)a] > cost[(size_t)b]; });
+        using Load = std::pair<int64_t, int32_t>;
+        std::priority_queue<Load, std::vector<Load>, std::greater<Load>> heap;
+        for (int32_t w = 0; w < nw; ++w) heap.push({0, w});
+        std::vector<int32_t> warp_of((size_t)n);
+        for (int32_t r : ord) {
+            const Load top = heap.top();
+            heap.pop();
+            warp_of[(size_t)r] = top.second;
+            heap.push({top.first + cost[(size_t)r], top.second});
+        }
+        auto cls = [&](int32_t r) {
+            const uint32_t w = (uint32_t)S.slice[(size_t)(4 * r + 3)];
+            if (w == 0) return 0;
+            const int q = (int)(w >> 24);
+            if (q == 0) return 2;
+            return q % dev::kSubSeg == 0 ? 1 : 0;
+        };
+        std::vector<int32_t> seq((size_t)n);
+        std::iota(seq.begin(), seq.end(), 0);
+        std::stable_sort(seq.begin(), seq.end(), [&](int32_t a, int32_t b) {
+            if (warp_of[(size_t)a] != warp_of[(size_t)b]) return warp_of[(size_t)a] < warp_of[(size_t)b];
+            return cls(a) < cls(b);
+        });
+        std::vector<int32_t> start((size_t)nw + 1, 0);
+        for (int32_t r : seq) ++start[(size_t)warp_of[(size_t)r] + 1];
+        for (int32_t w = 0; w < nw; ++w) start[(size_t)w + 1] += start[(size_t)w];
+        std::vector<int32_t> recs((size_t)n * 4), affs(S.aff.empty() ? 0 : (size_t)n * 2);
+        for (int64_t k = 0; k < n; ++k) {
+            const size_t r = (size_t)seq[(size_t)k];
+            for (int q = 0; q < 4; ++q) recs[(size_t)k * 4 + q] = S.slice[r * 4 + q];
+            if (!affs.empty()) {
+                affs[(size_t)k * 2] = S.aff[r * 2];
+                affs[(size_t)k * 2 + 1] = S.aff[r * 2 + 1];
+            }
+        }
+        d.slice = reinterpret_cast<const int4*>(up(recs));
+        d.aff = affs.empty() ? nullptr : reinterpret_cast<const int2*>(up(affs));
+        d.start = up(start);
+        return d;
+    }
+
+    template <class T>
+    void attach_sched(dev::KParams<T>& Q, int ctas) {
+        auto it = scheds.find(ctas);
+        if (it == scheds.end()) {
+            Sched sc;
+            sc.a = build_sched(L.A, ctas * dev::kWarps);
+            sc.at = build_sched(L.AT, ctas * dev::kWarps);
+            cuda_ok(cudaStreamSynchronize(stream), "schedule upload");
+            it = scheds.emplace(ctas, sc).first;
+        }
+        Q.a_wslice = it->second.a.slice;
+        Q.a_waff = it->second.a.aff;
+        Q.a_wstart = it->second.a.start;
+        Q.t_wslice = it->second.at.slice;
+        Q.t_waff = it->second.at.aff;
+        Q.t_wstart = it->second.at.start;
     }
 
     // split-slice arrival counters start every product at zero (an abandoned
@@ -362,7 +458,9 @@ struct EngineImpl {
         }
         dev::GridArgs gg = ga;
         gg.svec_bytes = sizeof(T) == 4 ? ystage_f : ystage_d;
-        void* args[] = {(void*)&P, (void*)&gg};
+        dev::KParams<T> Q = P;
+        attach_sched(Q, ctas);
+        void* args[] = {(void*)&Q, (void*)&gg};
         cuda_ok(cudaLaunchCooperativeKernel((const void*)dev::k_pdlp<T, V>, dim3(ctas), dim3(dev::kBlock), args,
                                             (size_t)gg.svec_bytes, st),
                 "cudaLaunchCooperativeKernel");
