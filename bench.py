@@ -431,7 +431,7 @@ def batch_shapes(name, count=0, m_hi=0, world=1):
 def make_batch(B, name, count=0, m_hi=0, world=1, rank=0):
     """This rank's share of the batch (all of it on one GPU), balanced by load."""
     shapes = batch_shapes(name, count, m_hi, world)
-    mine = my_share(B, [B.request_work(m, n, n * k) for (m, n, k, _) in shapes], world, rank)
+    mine = my_share(B, [B.request_cost(m, n, n * k) for (m, n, k, _) in shapes], world, rank)
     probs = []
     for i in mine:
         m, n, k, seed = shapes[i]
@@ -540,7 +540,7 @@ def serve_bench(args, world, rank, local):
     # the offered rate grows with the GPUs (weak scaling); each rank serves its
     # share of the one stream, routed in arrival order to the least-loaded rank
     full = serve_stream(p["rate"] * world, args.serve_seconds or p["seconds"], p["seed"])
-    mine = my_share(B, [B.request_work(m, n, n * k) for (_, m, n, k, _) in full], world, rank, online=True)
+    mine = my_share(B, [B.request_cost(m, n, n * k) for (_, m, n, k, _) in full], world, rank, online=True)
     stream = [full[i] for i in mine]
     t0 = time.time()
     lps = [B.gen_random_lp(m, n, k, sd, True) for (_, m, n, k, sd) in stream]

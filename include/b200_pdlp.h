@@ -364,6 +364,14 @@ void b2_server_destroy(b2_server* s);
  * elements one PDHG attempt passes over (both products, both vector passes). */
 int64_t b2_request_work(int32_t m, int32_t n, int64_t nnz);
 
+/* The expected cost of a whole solve, for shares of a batch or a stream:
+ * b2_request_work times the attempts an LP of m rows takes to 1e-6, modelled
+ * as round(167 m^0.657) (a fit over the 4,096 LPs of the uneven batch family,
+ * m 50..5,000). Larger LPs need more attempts as well as more work per
+ * attempt, so shares planned on this cost end together more closely than
+ * shares planned on the work of one attempt. */
+int64_t b2_request_cost(int32_t m, int32_t n, int64_t nnz);
+
 /* Assigns `count` items of load work[i] >= 0 to `parts` shares; rank_of[i]
  * receives item i's share. online = 0 (a batch known up front): items by
  * decreasing load (equal loads by index), each to the least-loaded share

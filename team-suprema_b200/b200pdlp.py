@@ -46,7 +46,7 @@ EXPORTED = [
     "b2_server_stats_get", "b2_pdlp_form_build", "b2_pdlp_form_view", "b2_pdlp_form_extract",
     "b2_pdlp_form_destroy", "b2_presolve", "b2_presolved_view", "b2_postsolve", "b2_presolved_destroy",
     "b2_server_destroy", "b2_lp_write", "b2_lp_read_dims", "b2_lp_read",
-    "b2_layout_digest", "b2_layout_get_stats", "b2_request_work", "b2_shard_plan", "b2_pool_create", "b2_pool_submit", "b2_pool_submit_file",
+    "b2_layout_digest", "b2_layout_get_stats", "b2_request_work", "b2_request_cost", "b2_shard_plan", "b2_pool_create", "b2_pool_submit", "b2_pool_submit_file",
     "b2_pool_wait", "b2_pool_stats_get", "b2_pool_destroy",
     "b2_scale", "b2_scale_gpu",
     "b2_gen_random_lp", "b2_gen_transport", "b2_last_error", "b2_version",
@@ -206,6 +206,8 @@ def lib():
                                            C.POINTER(C.c_uint64)]
             L.b2_request_work.argtypes = [i32, i32, i64]
             L.b2_request_work.restype = i64
+            L.b2_request_cost.argtypes = [i32, i32, i64]
+            L.b2_request_cost.restype = i64
             L.b2_shard_plan.argtypes = [vp, i64, i32, i32, vp]
             L.b2_pool_create.argtypes = [vp, i32, C.POINTER(ServerOpts), C.POINTER(SolveOpts), C.POINTER(vp)]
             L.b2_pool_submit.argtypes = [vp, C.POINTER(_LPView), C.POINTER(i64)]
@@ -632,6 +634,12 @@ def layout_stats(unscaled_form: RangedLP, scaled_form: RangedLP, Dr, Dc, whole_g
 def request_work(m: int, n: int, nnz: int) -> int:
     """The load unit of sharding and routing: 2 nnz + m + n (b2_request_work)."""
     return int(lib().b2_request_work(int(m), int(n), int(nnz)))
+
+
+def request_cost(m: int, n: int, nnz: int) -> int:
+    """Expected cost of a whole solve: request_work x round(167 m^0.657)
+    attempts (b2_request_cost), the load of batch and stream shares."""
+    return int(lib().b2_request_cost(int(m), int(n), int(nnz)))
 
 
 def shard_plan(work, parts: int, online: bool = False) -> np.ndarray:

@@ -342,6 +342,8 @@ int b2_layout_get_stats(const b2_lp_view* U, const b2_lp_view* S, const double* 
 
 int64_t b2_request_work(int32_t m, int32_t n, int64_t nnz) { return b2::request_work(m, n, nnz); }
 
+int64_t b2_request_cost(int32_t m, int32_t n, int64_t nnz) { return b2::request_cost(m, n, nnz); }
+
 int b2_shard_plan(const int64_t* work, int64_t count, int32_t parts, int32_t online, int32_t* rank_of) {
     return b2::guarded([&] { b2::shard_plan(work, count, parts, online != 0, rank_of); });
 }

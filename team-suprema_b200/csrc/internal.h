@@ -193,6 +193,7 @@ int64_t server_backlog(ServerImpl* s);  // b2_server_stats.backlog_work
 
 // Shares over several GPUs (pool.cpp). All functions throw Error.
 int64_t request_work(int32_t m, int32_t n, int64_t nnz);
+int64_t request_cost(int32_t m, int32_t n, int64_t nnz);
 void shard_plan(const int64_t* work, int64_t count, int32_t parts, bool online, int32_t* rank_of);
 struct PoolImpl;
 PoolImpl* pool_create(const int32_t* devices, int32_t count, const b2_server_opts& so, const b2_solve_opts& o);

@@ -17,7 +17,7 @@ import torch
 import torch.multiprocessing as mp
 
 import b200pdlp as B
-from conftest import ROOT
+from conftest import GOLDEN, ROOT
 
 sys.path.insert(0, ROOT)
 
@@ -91,9 +91,9 @@ def _rank_main(rank, world, port, out):
     import b200pdlp as B_
     w, r, _ = bench.dist_setup(world)
     shapes = bench.batch_shapes("batch", 96, 0, w)
-    batch = bench.my_share(B_, [B_.request_work(m, n, n * k) for (m, n, k, _) in shapes], w, r)
+    batch = bench.my_share(B_, [B_.request_cost(m, n, n * k) for (m, n, k, _) in shapes], w, r)
     full = bench.serve_stream(2000.0 * w, 0.05, 0)
-    stream = bench.my_share(B_, [B_.request_work(m, n, n * k) for (_, m, n, k, _) in full], w, r, online=True)
+    stream = bench.my_share(B_, [B_.request_cost(m, n, n * k) for (_, m, n, k, _) in full], w, r, online=True)
     total = bench.dist_sum(float(len(batch)), w)
     out[rank] = (batch, stream, len(shapes), len(full), total)
     import torch.distributed as dist
@@ -115,3 +115,38 @@ def test_two_gloo_ranks_take_disjoint_covering_shares():
     work = np.array([B.request_work(m, n, n * k) for (m, n, k, _) in shapes])
     l0, l1 = work[b0].sum(), work[b1].sum()
     assert abs(l0 - l1) <= work.max()
+
+
+def test_request_cost_model_and_measured_batch_shares():
+    """b2_request_cost = work x round(167 m^0.657). The attempts each LP of the
+    4,096-LP batch took on a B200 (tests/golden/batch_attempts.csv, made by
+    make_batch_attempts.py) give each LP's measured cost, work x attempts.
+    The model's attempts follow the measured ones; shares of the whole batch
+    planned on either load end within 5 % of each other; shares of smaller
+    batches (256 LPs over 8 GPUs, averaged over 20 draws) end closer together
+    when planned on the cost."""
+    for (m, n, z) in ((1, 1, 1), (100, 300, 2000), (5000, 15000, 100000)):
+        assert B.request_cost(m, n, z) == B.request_work(m, n, z) * round(167.0 * m ** 0.657)
+    assert B.request_cost(0, 0, 0) == 0
+    rows = np.loadtxt(os.path.join(GOLDEN, "batch_attempts.csv"), delimiter=",", skiprows=1, dtype=np.int64)
+    assert rows.shape == (4096, 4)
+    m, n, z, att = rows.T
+    assert att.min() > 0
+    measured = ((2 * z + m + n) * att).astype(np.float64)
+    model = 167.0 * m.astype(np.float64) ** 0.657
+    assert np.corrcoef(np.log(model), np.log(att))[0, 1] > 0.85
+    work = np.array([B.request_work(int(a), int(b), int(c)) for a, b, c in zip(m, n, z)], np.int64)
+    cost = np.array([B.request_cost(int(a), int(b), int(c)) for a, b, c in zip(m, n, z)], np.int64)
+
+    def spread(load, idx, parts):
+        got = np.bincount(B.shard_plan(load[idx], parts), weights=measured[idx], minlength=parts)
+        return got.max() / got.mean()
+
+    everything = np.arange(4096)
+    for parts in (2, 4, 8):
+        assert spread(work, everything, parts) < 1.05 and spread(cost, everything, parts) < 1.05
+    rng = np.random.default_rng(0)
+    draws = [rng.choice(4096, 256, replace=False) for _ in range(20)]
+    by_work = np.mean([spread(work, d, 8) for d in draws])
+    by_cost = np.mean([spread(cost, d, 8) for d in draws])
+    assert by_cost < by_work, (by_cost, by_work)
