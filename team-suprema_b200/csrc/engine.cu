@@ -175,7 +175,9 @@ struct EngineImpl {
 
     // Work-balanced order of the slice records over the grid's warps, for the
     // whole-grid kernel's rows and columns passes: the records, costliest
-    // first (unroll rounds of their steps plus a fixed share), each go to the
+    // first (a plain record: its steps, each a row of 32 gathers, plus 4 for
+    // the record and its epilogue; a dense-run record, whose loads go out 8
+    // steps at a time: its rounds plus 2), each go to the
     // least-loaded warp (ties: the lowest warp), so that no warp holds a much
     // longer chain of records than the average. A warp's records then run in
     // an order that keeps split groups free of cycles of waits: records that
@@ -202,7 +204,7 @@ struct EngineImpl {
             const int64_t len = (int64_t)((uint32_t)S.slice[(size_t)(4 * r + 1)] & kLenMask);
             const bool dense = !S.aff.empty() && S.aff[(size_t)(2 * r)] >= 0;
             const int64_t u = dense ? dev::kDenseUnroll : dev::kUnroll;
-            cost[(size_t)r] = (len + u - 1) / u + 2;
+            cost[(size_t)r] = dense ? (len + u - 1) / u + 2 : len + 4;
         }
         std::vector<int32_t> ord((size_t)n);
         std::iota(ord.begin(), ord.end(), 0);
