@@ -173,18 +173,13 @@ struct EngineImpl {
         if (stream) cudaStreamDestroy(stream);
     }
 
-    // Work-balanced order of the slice records over the grid's warps, for the
-    // whole-grid kernel's rows and columns passes: the records, costliest
-    // first (a plain record: its steps, each a row of 32 gathers, plus 4 for
-    // the record and its epilogue; a dense-run record, whose loads go out 8
-    // steps at a time: its rounds plus 2), each go to the
-    // least-loaded warp (ties: the lowest warp), so that no warp holds a much
-    // longer chain of records than the average. A warp's records then run in
-    // an order that keeps split groups free of cycles of waits: records that
-    // wait for nothing (unsplit slices, subgroup members) first, then
-    // subgroup leaders, then group owners, each in record order. A leader
-    // waits only for members and an owner only for members and leaders, so
-    // every wait ends. Deterministic: a function of the layout and the grid.
+    // The whole-grid kernel's rows and columns passes run the slice records
+    // on a work-balanced schedule over the grid's warps (schedule_records:
+    // costliest first to the least-loaded warp; inside a warp, records that
+    // wait for nothing first, then subgroup leaders, then group owners, so
+    // every wait ends). The records are copied into that order, once per grid
+    // size; the schedule is a function of the layout and the grid, so solves
+    // stay deterministic.
     struct SchedDev {
         const int4* slice = nullptr;
         const int2* aff = nullptr;
@@ -199,42 +194,8 @@ struct EngineImpl {
         SchedDev d;
         const int64_t n = S.n_slices();
         if (n == 0 || nw <= 1) return d;
-        std::vector<int64_t> cost((size_t)n);
-        for (int64_t r = 0; r < n; ++r) {
-            const int64_t len = (int64_t)((uint32_t)S.slice[(size_t)(4 * r + 1)] & kLenMask);
-            const bool dense = !S.aff.empty() && S.aff[(size_t)(2 * r)] >= 0;
-            const int64_t u = dense ? dev::kDenseUnroll : dev::kUnroll;
-            cost[(size_t)r] = dense ? (len + u - 1) / u + 2 : len + 4;
-        }
-        std::vector<int32_t> ord((size_t)n);
-        std::iota(ord.begin(), ord.end(), 0);
-        std::stable_sort(ord.begin(), ord.end(), [&](int32_t a, int32_t b) { return cost[(size_t)a] > cost[(size_t)b]; });
-        using Load = std::pair<int64_t, int32_t>;
-        std::priority_queue<Load, std::vector<Load>, std::greater<Load>> heap;
-        for (int32_t w = 0; w < nw; ++w) heap.push({0, w});
-        std::vector<int32_t> warp_of((size_t)n);
-        for (int32_t r : ord) {
-            const Load top = heap.top();
-            heap.pop();
-            warp_of[(size_t)r] = top.second;
-            heap.push({top.first + cost[(size_t)r], top.second});
-        }
-        auto cls = [&](int32_t r) {
-            const uint32_t w = (uint32_t)S.slice[(size_t)(4 * r + 3)];
-            if (w == 0) return 0;
-            const int q = (int)(w >> 24);
-            if (q == 0) return 2;
-            return q % dev::kSubSeg == 0 ? 1 : 0;
-        };
-        std::vector<int32_t> seq((size_t)n);
-        std::iota(seq.begin(), seq.end(), 0);
-        std::stable_sort(seq.begin(), seq.end(), [&](int32_t a, int32_t b) {
-            if (warp_of[(size_t)a] != warp_of[(size_t)b]) return warp_of[(size_t)a] < warp_of[(size_t)b];
-            return cls(a) < cls(b);
-        });
-        std::vector<int32_t> start((size_t)nw + 1, 0);
-        for (int32_t r : seq) ++start[(size_t)warp_of[(size_t)r] + 1];
-        for (int32_t w = 0; w < nw; ++w) start[(size_t)w + 1] += start[(size_t)w];
+        std::vector<int32_t> seq, start;
+        schedule_records(S, nw, dev::kDenseUnroll, dev::kSubSeg, seq, start);
         std::vector<int32_t> recs((size_t)n * 4), affs(S.aff.empty() ? 0 : (size_t)n * 2);
         for (int64_t k = 0; k < n; ++k) {
             const size_t r = (size_t)seq[(size_t)k];

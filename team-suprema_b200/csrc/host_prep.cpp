@@ -9,6 +9,7 @@
 #include <cstring>
 #include <limits>
 #include <numeric>
+#include <queue>
 #include <string>
 #include <thread>
 #include <vector>
@@ -521,6 +522,47 @@ void build_layout(const b2_lp_view& U, const b2_lp_view& S, const double* Dr, co
     L.denom_p = 1.0 + std::max(finite_inf_norm(U.rL, m), finite_inf_norm(U.rU, m));
     L.denom_d = 1.0 + finite_inf_norm(U.c, n);
     L.obj_offset = U.obj_offset;
+}
+
+void schedule_records(const SellHost& S, int warps, int dense_unroll, int sub_seg, std::vector<int32_t>& seq,
+                      std::vector<int32_t>& start) {
+    const int64_t n = S.n_slices();
+    if (warps < 1 || dense_unroll < 1 || sub_seg < 1) fail(B2_ERR_INVALID, "schedule: bad arguments");
+    std::vector<int64_t> cost((size_t)n);
+    for (int64_t r = 0; r < n; ++r) {
+        const int64_t len = (int64_t)((uint32_t)S.slice[(size_t)(4 * r + 1)] & kLenMask);
+        const bool dense = !S.aff.empty() && S.aff[(size_t)(2 * r)] >= 0;
+        cost[(size_t)r] = dense ? (len + dense_unroll - 1) / dense_unroll + 2 : len + 4;
+    }
+    std::vector<int32_t> ord((size_t)n);
+    std::iota(ord.begin(), ord.end(), 0);
+    std::stable_sort(ord.begin(), ord.end(), [&](int32_t a, int32_t b) { return cost[(size_t)a] > cost[(size_t)b]; });
+    using Load = std::pair<int64_t, int32_t>;
+    std::priority_queue<Load, std::vector<Load>, std::greater<Load>> heap;
+    for (int32_t w = 0; w < warps; ++w) heap.push({0, w});
+    std::vector<int32_t> warp_of((size_t)n);
+    for (int32_t r : ord) {
+        const Load top = heap.top();
+        heap.pop();
+        warp_of[(size_t)r] = top.second;
+        heap.push({top.first + cost[(size_t)r], top.second});
+    }
+    auto cls = [&](int32_t r) {
+        const uint32_t w = (uint32_t)S.slice[(size_t)(4 * r + 3)];
+        if (w == 0) return 0;
+        const int q = (int)(w >> 24);
+        if (q == 0) return 2;
+        return q % sub_seg == 0 ? 1 : 0;
+    };
+    seq.resize((size_t)n);
+    std::iota(seq.begin(), seq.end(), 0);
+    std::stable_sort(seq.begin(), seq.end(), [&](int32_t a, int32_t b) {
+        if (warp_of[(size_t)a] != warp_of[(size_t)b]) return warp_of[(size_t)a] < warp_of[(size_t)b];
+        return cls(a) < cls(b);
+    });
+    start.assign((size_t)warps + 1, 0);
+    for (int32_t r : seq) ++start[(size_t)warp_of[(size_t)r] + 1];
+    for (int32_t w = 0; w < warps; ++w) start[(size_t)w + 1] += start[(size_t)w];
 }
 
 // FNV-1a over every array and scalar of a layout: two layouts with the same

@@ -96,6 +96,17 @@ void build_layout(const b2_lp_view& U, const b2_lp_view& S, const double* Dr, co
                   const BuildParams& bp, Layout& L);
 uint64_t layout_digest(const Layout& L);
 
+// The whole-grid kernel's work-balanced order of a matrix's slice records
+// over `warps` warps: seq holds the record indices, warp w's records at
+// seq[start[w] .. start[w + 1]). Records go costliest first to the
+// least-loaded warp (ties: the lowest); a plain record costs its steps + 4, a
+// dense-run record ceil(steps / dense_unroll) + 2. Inside a warp: records
+// that wait for nothing (unsplit, subgroup members) first, then subgroup
+// leaders (segment % sub_seg == 0), then group owners (segment 0), each in
+// record order.
+void schedule_records(const SellHost& S, int warps, int dense_unroll, int sub_seg, std::vector<int32_t>& seq,
+                      std::vector<int32_t>& start);
+
 // Ruiz + Pock-Chambolle on the host; the same bits with any number of threads.
 void scale_lp(const b2_lp_view& lp, int ruiz_passes, double* val_s, double* c_s, double* rL_s, double* rU_s,
               double* l_s, double* u_s, double* Dr, double* Dc, int threads = 1);
