@@ -228,7 +228,8 @@ __device__ __forceinline__ T ld_it(const T* p) {
 // One-dimensional bulk copy (TMA engine) from this GPU's global memory into
 // this CTA's shared memory, completed on an mbarrier: the issuing thread
 // announces the bytes (arrive.expect_tx) and the copy counts them off. Both
-// addresses 16-byte aligned, bytes a multiple of 16. No multicast.
+// addresses 16-byte aligned, bytes a multiple of 16; the copy lands in this
+// CTA's shared memory only.
 __device__ __forceinline__ uint32_t smem_addr(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
 __device__ __forceinline__ void mbar_init(unsigned long long* bar, unsigned count) {
     asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(bar)), "r"(count) : "memory");
