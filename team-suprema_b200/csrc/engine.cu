@@ -327,7 +327,10 @@ struct EngineImpl {
         auto stage = [&](const void* fn, size_t elem) -> int {
             const size_t bytes = ((size_t)L.m * elem + 15) / 16 * 16;
             if (L.m == 0 || bytes > dev::kYStageMax) return 0;
-            if (cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes) != cudaSuccess) {
+            // the kernel's limit is process-wide: every engine sets the same
+            // largest size, so one engine's set-up never lowers another's
+            if (cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dev::kYStageMax) !=
+                cudaSuccess) {
                 cudaGetLastError();
                 return 0;
             }
